@@ -1,0 +1,525 @@
+// C ABI of libdrpt_gpu.so and the host orchestration of the k-NN-graph path
+// (MDRPT::grow_trees + MDRPT::gather_nns, mdrpt.cpp:46-121, 273-291).
+//
+// Data layout in HBM for n points, T trees, global depth gd:
+//   X            n x d row-major (f32 or u8), read by K1 and gathered by K6
+//   P            (T*(gd-1)) x n column-major: the split value of every point
+//                for tree t at level l is column t*(gd-1)+l (the reference
+//                computes gd columns per tree and never splits on the last)
+//   ord / val    T x n ping-pong: point ids grouped by node, and their values
+//   off          T x (nodes+1) node starts per level
+//   final_order  T x n point ids grouped by final leaf, final_off leaf starts
+//   cand         n x T x nn per-tree nearest lists (dist f32 + idx i32)
+//   out          n x nn merged lists
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "host_algo.h"
+#include "kernels.cuh"
+
+struct drpt_ctx {
+  int device = 0;
+  struct Buf {
+    void *p = nullptr;
+    size_t bytes = 0;
+  };
+  std::map<std::string, Buf> bufs;
+  std::map<std::pair<int64_t, int>, std::pair<std::vector<int32_t>, std::vector<int32_t>>> perms;
+  cudaEvent_t ev[8] = {};
+  int launches = 0;
+};
+
+namespace drpt {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+namespace {
+
+template <typename T>
+drpt_status ws_get(drpt_ctx *c, const char *name, size_t count, T **out) {
+  const size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+  drpt_ctx::Buf &b = c->bufs[name];
+  if (b.bytes < bytes) {
+    if (b.p) DRPT_CUDA(cudaFree(b.p));
+    b.p = nullptr;
+    b.bytes = 0;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+      b.p = nullptr;
+      set_error("cudaMalloc(%zu) for %s: %s", bytes, name, cudaGetErrorString(e));
+      return DRPT_ERR_OOM;
+    }
+    b.bytes = bytes;
+  }
+  *out = (T *)b.p;
+  return DRPT_OK;
+}
+
+struct Geometry {
+  int td, gd, nleaf;
+};
+
+drpt_status geometry(int64_t n, int tree_depth, double ratio, Geometry *g) {
+  g->td = tree_depth > 0 ? tree_depth : (int)(std::log2((double)n) - 2);  // main.cpp:143
+  g->gd = (int)(g->td * ratio);                                          // mdrpt.cpp:52
+  if (g->gd <= 0 || g->gd > std::log2((double)n)) {                       // drpt_global.cpp:155-158
+    set_error("global tree depth %d outside [1, log2(%lld)]", g->gd, (long long)n);
+    return DRPT_ERR_DEPTH_OUT_OF_RANGE;
+  }
+  if (g->gd > 30) {
+    set_error("global tree depth %d too large", g->gd);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  g->nleaf = 1 << (g->gd - 1);
+  return DRPT_OK;
+}
+
+// K1 with the CSC of the used columns of B built on the host.
+drpt_status project_cols(drpt_ctx *c, const void *X, int dtype, int64_t n, int d, const float *B,
+                         int L, const std::vector<int32_t> &cols, float *P, cudaStream_t s) {
+  const int ncols = (int)cols.size();
+  std::vector<int32_t> colptr(ncols + 1, 0), row;
+  std::vector<float> val;
+  for (int q = 0; q < ncols; ++q) {
+    for (int k = 0; k < d; ++k) {
+      const float b = B[(int64_t)k * L + cols[q]];
+      if (b != 0.0f) {
+        row.push_back(k);
+        val.push_back(b);
+      }
+    }
+    colptr[q + 1] = (int32_t)row.size();
+  }
+  int32_t *dcol, *drow;
+  float *dval;
+  DRPT_TRY(ws_get(c, "csc_colptr", colptr.size(), &dcol));
+  DRPT_TRY(ws_get(c, "csc_row", std::max<size_t>(row.size(), 1), &drow));
+  DRPT_TRY(ws_get(c, "csc_val", std::max<size_t>(val.size(), 1), &dval));
+  // Pageable sources: the copies complete before these calls return.
+  DRPT_CUDA(cudaMemcpyAsync(dcol, colptr.data(), colptr.size() * 4, cudaMemcpyHostToDevice, s));
+  if (!row.empty()) {
+    DRPT_CUDA(cudaMemcpyAsync(drow, row.data(), row.size() * 4, cudaMemcpyHostToDevice, s));
+    DRPT_CUDA(cudaMemcpyAsync(dval, val.data(), val.size() * 4, cudaMemcpyHostToDevice, s));
+  }
+  CscDev csc{dcol, drow, dval, ncols};
+  DRPT_TRY(launch_project(X, dtype, n, d, csc, P, s));
+  c->launches += 1;
+  return DRPT_OK;
+}
+
+// Global trees of all T trees; returns pointers to the final order/offsets
+// (inside the workspace).
+drpt_status global_trees(drpt_ctx *c, const float *P, int64_t n, int T, int gd, int exact,
+                         float *medians, int32_t **order_out, int32_t **off_out, cudaStream_t s) {
+  const int nleaf = 1 << (gd - 1);
+  int32_t *ord[2], *off[2];
+  float *val[2];
+  DRPT_TRY(ws_get(c, "ord_a", (size_t)T * n, &ord[0]));
+  DRPT_TRY(ws_get(c, "ord_b", (size_t)T * n, &ord[1]));
+  DRPT_TRY(ws_get(c, "val_a", (size_t)T * n, &val[0]));
+  DRPT_TRY(ws_get(c, "val_b", (size_t)T * n, &val[1]));
+  DRPT_TRY(ws_get(c, "off_a", (size_t)T * (nleaf + 1), &off[0]));
+  DRPT_TRY(ws_get(c, "off_b", (size_t)T * (nleaf + 1), &off[1]));
+  if (gd == 1) {
+    // One global leaf holding every point in index order.
+    std::vector<int32_t> iota(n), o(2 * T);
+    for (int64_t i = 0; i < n; ++i) iota[i] = (int32_t)i;
+    for (int t = 0; t < T; ++t) {
+      o[2 * t] = 0;
+      o[2 * t + 1] = (int32_t)n;
+      DRPT_CUDA(cudaMemcpyAsync(ord[0] + (size_t)t * n, iota.data(), n * 4, cudaMemcpyHostToDevice, s));
+    }
+    DRPT_CUDA(cudaMemcpyAsync(off[0], o.data(), o.size() * 4, cudaMemcpyHostToDevice, s));
+    *order_out = ord[0];
+    *off_out = off[0];
+    return DRPT_OK;
+  }
+  int cur = 0;
+  for (int level = 0; level < gd - 1; ++level) {
+    LevelArgs a;
+    a.P = P;
+    a.n = n;
+    a.T = T;
+    a.gd = gd;
+    a.level = level;
+    a.ord_in = level == 0 ? nullptr : ord[cur];
+    a.val_in = level == 0 ? P : val[cur];
+    a.off_in = level == 0 ? nullptr : off[cur];
+    a.ord_out = ord[cur ^ 1];
+    a.val_out = level + 1 < gd - 1 ? val[cur ^ 1] : nullptr;
+    a.off_out = off[cur ^ 1];
+    a.medians = medians;
+    a.exact = exact;
+    DRPT_TRY(launch_level(a, s));
+    c->launches += 1;
+    cur ^= 1;
+  }
+  *order_out = ord[cur];
+  *off_out = off[cur];
+  return DRPT_OK;
+}
+
+struct LocalPlan {
+  int ld = 0;
+  int64_t min_leaf = 0;
+  int64_t sum_sq = 0;
+  int max_leaf = 0;
+};
+
+// Host part of the local split: leaf sizes -> local depth, the reference's
+// error conditions, permutation tables; then K5.
+drpt_status local_phase(drpt_ctx *c, const int32_t *order, const int32_t *goff, int64_t n, int T,
+                        int gd, int nn, int local_tree_offset, int forced_ld, int exact,
+                        const uint32_t *local_seeds, int d, int32_t *final_order,
+                        int32_t *final_off, LocalPlan *plan, cudaStream_t s) {
+  const int nleaf = 1 << (gd - 1);
+  std::vector<int32_t> h_off((size_t)T * (nleaf + 1));
+  DRPT_CUDA(cudaMemcpyAsync(h_off.data(), goff, h_off.size() * 4, cudaMemcpyDeviceToHost, s));
+  DRPT_CUDA(cudaStreamSynchronize(s));
+  int64_t min_leaf = INT32_MAX;
+  bool empty = false;
+  for (int t = 0; t < T; ++t)
+    for (int j = 0; j < nleaf; ++j) {
+      const int64_t sz = h_off[(size_t)t * (nleaf + 1) + j + 1] - h_off[(size_t)t * (nleaf + 1) + j];
+      if (sz == 0) empty = true;
+      else min_leaf = std::min(min_leaf, sz);
+    }
+  plan->min_leaf = min_leaf;
+  int ld = forced_ld;
+  if (ld <= 0)  // mdrpt.cpp:324
+    ld = (int)(std::log2((double)(int)min_leaf) - (std::log2((double)nn) + local_tree_offset));
+  plan->ld = ld;
+  if (ld <= 0) {  // drpt_local.cpp:84-88
+    set_error("local tree depth %d <= 0 (smallest global leaf %lld, nn %d)", ld,
+              (long long)min_leaf, nn);
+    return DRPT_ERR_DEPTH_OUT_OF_RANGE;
+  }
+  if (empty) {
+    set_error("a global leaf is empty (the reference throws from DRPTLocal)");
+    return DRPT_ERR_EMPTY_LEAF;
+  }
+  if (ld > 24 || (int64_t)nleaf << ld > INT32_MAX) {
+    set_error("local tree depth %d too large", ld);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  for (int t = 0; t < T; ++t)
+    for (int j = 0; j < nleaf; ++j) {
+      const int64_t sz = h_off[(size_t)t * (nleaf + 1) + j + 1] - h_off[(size_t)t * (nleaf + 1) + j];
+      if (ld > std::log2((double)sz)) {
+        set_error("local tree depth %d > log2(%lld)", ld, (long long)sz);
+        return DRPT_ERR_DEPTH_OUT_OF_RANGE;
+      }
+    }
+  if (exact && local_seeds) {
+    for (int t = 0; t < T; ++t)
+      if (!host_local_matrix_is_zero(local_seeds[t], d, ld)) {
+        set_error("local projection matrix of tree %d is not all zero", t);
+        return DRPT_ERR_LOCAL_MATRIX_NONZERO;
+      }
+  }
+  // Permutations per distinct size, appended to one pool.
+  std::vector<int32_t> pool;
+  std::vector<int64_t> pbase((size_t)T * nleaf), fbase((size_t)T * nleaf);
+  std::map<int64_t, std::pair<int64_t, int64_t>> where;
+  int64_t sum_sq = 0;
+  int max_leaf = 0;
+  for (int t = 0; t < T; ++t)
+    for (int j = 0; j < nleaf; ++j) {
+      const int64_t sz = h_off[(size_t)t * (nleaf + 1) + j + 1] - h_off[(size_t)t * (nleaf + 1) + j];
+      auto it = where.find(sz);
+      if (it == where.end()) {
+        auto key = std::make_pair(sz, ld);
+        auto ct = c->perms.find(key);
+        if (ct == c->perms.end()) {
+          std::vector<int32_t> perm, first;
+          host_local_permutation(sz, ld, perm, first);
+          ct = c->perms.emplace(key, std::make_pair(std::move(perm), std::move(first))).first;
+        }
+        const int64_t pb = (int64_t)pool.size();
+        pool.insert(pool.end(), ct->second.first.begin(), ct->second.first.end());
+        const int64_t fb = (int64_t)pool.size();
+        pool.insert(pool.end(), ct->second.second.begin(), ct->second.second.end());
+        it = where.emplace(sz, std::make_pair(pb, fb)).first;
+      }
+      pbase[(size_t)t * nleaf + j] = it->second.first;
+      fbase[(size_t)t * nleaf + j] = it->second.second;
+      const int32_t *first = pool.data() + it->second.second;
+      for (int l = 0; l < (1 << ld); ++l) {
+        const int64_t m = first[l + 1] - first[l];
+        sum_sq += m * m;
+        max_leaf = std::max<int>(max_leaf, (int)m);
+      }
+    }
+  plan->sum_sq = sum_sq;
+  plan->max_leaf = max_leaf;
+  int32_t *dpool;
+  int64_t *dpb, *dfb;
+  DRPT_TRY(ws_get(c, "perm_pool", pool.size(), &dpool));
+  DRPT_TRY(ws_get(c, "perm_base", pbase.size(), &dpb));
+  DRPT_TRY(ws_get(c, "first_base", fbase.size(), &dfb));
+  DRPT_CUDA(cudaMemcpyAsync(dpool, pool.data(), pool.size() * 4, cudaMemcpyHostToDevice, s));
+  DRPT_CUDA(cudaMemcpyAsync(dpb, pbase.data(), pbase.size() * 8, cudaMemcpyHostToDevice, s));
+  DRPT_CUDA(cudaMemcpyAsync(dfb, fbase.data(), fbase.size() * 8, cudaMemcpyHostToDevice, s));
+  LocalArgs la{order, goff, dpb, dfb, dpool, n, T, nleaf, ld, final_order, final_off};
+  DRPT_TRY(launch_local(la, s));
+  c->launches += 1;
+  return DRPT_OK;
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+drpt_status check_common(const drpt_build_desc *d) {
+  if (!d) return DRPT_ERR_INVALID_ARG;
+  if (d->n < 2 || d->n > INT32_MAX || d->d <= 0 || d->ntrees <= 0 || d->nn <= 0 ||
+      (d->dtype != DRPT_DTYPE_F32 && d->dtype != DRPT_DTYPE_U8) || !(d->tree_depth_ratio > 0) ||
+      (d->mode != DRPT_MODE_EXACT && d->mode != DRPT_MODE_FAST)) {
+    set_error("invalid descriptor (n=%lld d=%d ntrees=%d nn=%d dtype=%d mode=%d)",
+              (long long)d->n, d->d, d->ntrees, d->nn, d->dtype, d->mode);
+    return DRPT_ERR_INVALID_ARG;
+  }
+  if (d->nn > kMaxK) {
+    set_error("nn = %d larger than %d", d->nn, kMaxK);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  return DRPT_OK;
+}
+
+}  // namespace
+}  // namespace drpt
+
+using namespace drpt;
+
+extern "C" {
+
+const char *drpt_version(void) { return "drpt-b200 0.1.0 (sm_100a)"; }
+
+const char *drpt_last_error(void) { return g_err; }
+
+drpt_status drpt_ctx_create(drpt_ctx **ctx, int device) {
+  if (!ctx) return DRPT_ERR_INVALID_ARG;
+  *ctx = nullptr;
+  int count = 0;
+  DRPT_CUDA(cudaGetDeviceCount(&count));
+  if (device < 0 || device >= count) {
+    set_error("device %d not present (%d devices)", device, count);
+    return DRPT_ERR_INVALID_ARG;
+  }
+  DRPT_CUDA(cudaSetDevice(device));
+  drpt_ctx *c = new drpt_ctx();
+  c->device = device;
+  for (auto &e : c->ev) {
+    cudaError_t err = cudaEventCreate(&e);
+    if (err != cudaSuccess) {
+      set_error("cudaEventCreate: %s", cudaGetErrorString(err));
+      drpt_ctx_destroy(c);
+      return DRPT_ERR_CUDA;
+    }
+  }
+  *ctx = c;
+  return DRPT_OK;
+}
+
+void drpt_ctx_destroy(drpt_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  for (auto &kv : c->bufs)
+    if (kv.second.p) cudaFree(kv.second.p);
+  for (auto &e : c->ev)
+    if (e) cudaEventDestroy(e);
+  delete c;
+}
+
+drpt_status drpt_host_projection(uint32_t seed, int32_t d, int32_t L, float density, float *B) {
+  if (d <= 0 || L <= 0 || !B) return DRPT_ERR_INVALID_ARG;
+  host_projection_matrix(seed, d, L, density, B);
+  return DRPT_OK;
+}
+
+drpt_status drpt_build_graph(drpt_ctx *c, const drpt_build_desc *desc, const void *data,
+                             int32_t *out_idx, float *out_dist, drpt_stats *stats) {
+  if (!c || !data || !out_idx) return DRPT_ERR_INVALID_ARG;
+  DRPT_TRY(check_common(desc));
+  DRPT_CUDA(cudaSetDevice(c->device));
+  cudaStream_t s = (cudaStream_t)desc->stream;
+  const int64_t n = desc->n;
+  const int d = desc->d, T = desc->ntrees, nn = desc->nn;
+  const int exact = desc->mode == DRPT_MODE_EXACT;
+  Geometry g;
+  DRPT_TRY(geometry(n, desc->tree_depth, desc->tree_depth_ratio, &g));
+  const int L = g.gd * T;
+  const float density = (float)(desc->density == 0 ? 1.0 / std::sqrt((double)d) : desc->density);
+  const int launches0 = c->launches;
+  cudaEvent_t *ev = c->ev;
+  DRPT_CUDA(cudaEventRecord(ev[0], s));
+
+  // Input rows on the device.
+  const size_t esz = desc->dtype == DRPT_DTYPE_U8 ? 1 : 4;
+  const void *X = data;
+  if (!desc->data_on_device) {
+    void *xd;
+    DRPT_TRY(ws_get(c, "x", (size_t)n * d * esz, (uint8_t **)&xd));
+    DRPT_CUDA(cudaMemcpyAsync(xd, data, (size_t)n * d * esz, cudaMemcpyHostToDevice, s));
+    X = xd;
+  }
+
+  // K1: projection on the columns the global trees split on.
+  std::vector<float> B((size_t)d * L);
+  host_projection_matrix(desc->seed, d, L, density, B.data());
+  std::vector<int32_t> cols;
+  for (int t = 0; t < T; ++t)
+    for (int l = 0; l + 1 < g.gd; ++l) cols.push_back(t * g.gd + l);
+  float *P = nullptr;
+  DRPT_TRY(ws_get(c, "P", std::max<size_t>(cols.size(), 1) * n, &P));
+  if (!cols.empty()) DRPT_TRY(project_cols(c, X, desc->dtype, n, d, B.data(), L, cols, P, s));
+  DRPT_CUDA(cudaEventRecord(ev[1], s));
+
+  // K2-K4: global trees.
+  int32_t *order, *goff;
+  DRPT_TRY(global_trees(c, P, n, T, g.gd, exact, nullptr, &order, &goff, s));
+  DRPT_CUDA(cudaEventRecord(ev[2], s));
+
+  // K5: local split (one host round trip for the leaf sizes).
+  int32_t *forder, *foff;
+  DRPT_TRY(ws_get(c, "final_order", (size_t)T * n, &forder));
+  LocalPlan plan;
+  {
+    // final_off needs the local depth; size it for the largest possible.
+    int32_t *tmp;
+    DRPT_TRY(ws_get(c, "final_off", (size_t)T * (n + 1), &tmp));
+    foff = tmp;
+  }
+  DRPT_TRY(local_phase(c, order, goff, n, T, g.gd, nn, desc->local_tree_offset, 0, exact,
+                       desc->local_seeds, d, forder, foff, &plan, s));
+  const int n_final = g.nleaf << plan.ld;
+  DRPT_CUDA(cudaEventRecord(ev[3], s));
+
+  // K6: leaf brute force.
+  int32_t *cidx;
+  float *cdist;
+  DRPT_TRY(ws_get(c, "cand_idx", (size_t)n * T * nn, &cidx));
+  DRPT_TRY(ws_get(c, "cand_dist", (size_t)n * T * nn, &cdist));
+  LeafKnnArgs ka{X, desc->dtype, n, d, T, nn, forder, foff, n_final, cidx, cdist};
+  DRPT_TRY(launch_leaf_knn_exact(ka, s));
+  c->launches += 1;
+  DRPT_CUDA(cudaEventRecord(ev[4], s));
+
+  // K7: merge into the output.
+  int32_t *oi = out_idx;
+  float *od = out_dist;
+  if (!desc->out_on_device) {
+    DRPT_TRY(ws_get(c, "out_idx", (size_t)n * nn, &oi));
+    DRPT_TRY(ws_get(c, "out_dist", (size_t)n * nn, &od));
+  } else if (!od) {
+    DRPT_TRY(ws_get(c, "out_dist", (size_t)n * nn, &od));
+  }
+  DRPT_TRY(launch_merge(cidx, cdist, n, T, nn, oi, od, s));
+  c->launches += 1;
+  DRPT_CUDA(cudaEventRecord(ev[5], s));
+  if (!desc->out_on_device) {
+    DRPT_CUDA(cudaMemcpyAsync(out_idx, oi, (size_t)n * nn * 4, cudaMemcpyDeviceToHost, s));
+    if (out_dist)
+      DRPT_CUDA(cudaMemcpyAsync(out_dist, od, (size_t)n * nn * 4, cudaMemcpyDeviceToHost, s));
+  }
+  DRPT_CUDA(cudaEventRecord(ev[6], s));
+  if (stats || !desc->out_on_device) DRPT_CUDA(cudaEventSynchronize(ev[6]));
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->tree_depth = g.td;
+    stats->global_depth = g.gd;
+    stats->local_depth = plan.ld;
+    stats->n_global_leaves = g.nleaf;
+    stats->n_final_leaves = n_final;
+    stats->max_final_leaf = plan.max_leaf;
+    stats->min_global_leaf = plan.min_leaf;
+    stats->sum_leaf_sq = plan.sum_sq;
+    stats->kernels_launched = c->launches - launches0;
+    stats->ms_project = elapsed(ev[0], ev[1]);
+    stats->ms_global = elapsed(ev[1], ev[2]);
+    stats->ms_local = elapsed(ev[2], ev[3]);
+    stats->ms_leaf_knn = elapsed(ev[3], ev[4]);
+    stats->ms_merge = elapsed(ev[4], ev[5]);
+    stats->ms_total = elapsed(ev[0], ev[6]);
+  }
+  return DRPT_OK;
+}
+
+drpt_status drpt_project(drpt_ctx *c, const void *X, int64_t n, int32_t d, int32_t dtype,
+                         const float *B_host, int32_t L, const int32_t *cols_host, int32_t ncols,
+                         float *P, void *stream) {
+  if (!c || !X || !B_host || !cols_host || !P || n <= 0 || d <= 0 || L <= 0 || ncols <= 0 ||
+      (dtype != DRPT_DTYPE_F32 && dtype != DRPT_DTYPE_U8))
+    return DRPT_ERR_INVALID_ARG;
+  for (int q = 0; q < ncols; ++q)
+    if (cols_host[q] < 0 || cols_host[q] >= L) return DRPT_ERR_INVALID_ARG;
+  DRPT_CUDA(cudaSetDevice(c->device));
+  std::vector<int32_t> cols(cols_host, cols_host + ncols);
+  return project_cols(c, X, dtype, n, d, B_host, L, cols, P, (cudaStream_t)stream);
+}
+
+drpt_status drpt_global_trees(drpt_ctx *c, const float *P, int64_t n, int32_t T, int32_t gd,
+                              int32_t exact, int32_t *order, int32_t *offsets, float *medians,
+                              void *stream) {
+  if (!c || !P || !order || !offsets || n < 2 || n > INT32_MAX || T <= 0 || gd <= 0 || gd > 30)
+    return DRPT_ERR_INVALID_ARG;
+  DRPT_CUDA(cudaSetDevice(c->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  int32_t *o, *f;
+  DRPT_TRY(global_trees(c, P, n, T, gd, exact, medians, &o, &f, s));
+  DRPT_CUDA(cudaMemcpyAsync(order, o, (size_t)T * n * 4, cudaMemcpyDeviceToDevice, s));
+  DRPT_CUDA(cudaMemcpyAsync(offsets, f, (size_t)T * ((1 << (gd - 1)) + 1) * 4,
+                            cudaMemcpyDeviceToDevice, s));
+  return DRPT_OK;
+}
+
+drpt_status drpt_local_leaves(drpt_ctx *c, const int32_t *order, const int32_t *offsets, int64_t n,
+                              int32_t T, int32_t gd, int32_t ld, int32_t *final_order,
+                              int32_t *final_offsets, void *stream) {
+  if (!c || !order || !offsets || !final_order || !final_offsets || n < 2 || T <= 0 || gd <= 0 ||
+      gd > 30 || ld <= 0)
+    return DRPT_ERR_INVALID_ARG;
+  DRPT_CUDA(cudaSetDevice(c->device));
+  LocalPlan plan;
+  return local_phase(c, order, offsets, n, T, gd, 1, 0, ld, 0, nullptr, 0, final_order,
+                     final_offsets, &plan, (cudaStream_t)stream);
+}
+
+drpt_status drpt_leaf_knn(drpt_ctx *c, const void *X, int32_t dtype, int64_t n, int32_t d,
+                          int32_t T, const int32_t *final_order, const int32_t *final_offsets,
+                          int32_t n_final, int32_t k, int32_t *cand_idx, float *cand_dist,
+                          void *stream) {
+  if (!c || !X || !final_order || !final_offsets || !cand_idx || !cand_dist || n <= 0 || d <= 0 ||
+      T <= 0 || n_final <= 0 || (dtype != DRPT_DTYPE_F32 && dtype != DRPT_DTYPE_U8))
+    return DRPT_ERR_INVALID_ARG;
+  DRPT_CUDA(cudaSetDevice(c->device));
+  LeafKnnArgs ka{X, dtype, n, d, T, k, final_order, final_offsets, n_final, cand_idx, cand_dist};
+  return launch_leaf_knn_exact(ka, (cudaStream_t)stream);
+}
+
+drpt_status drpt_merge_candidates(drpt_ctx *c, const int32_t *cand_idx, const float *cand_dist,
+                                  int64_t n, int32_t T, int32_t k, int32_t *out_idx,
+                                  float *out_dist, void *stream) {
+  if (!c || !cand_idx || !cand_dist || !out_idx || !out_dist || n <= 0 || T <= 0)
+    return DRPT_ERR_INVALID_ARG;
+  DRPT_CUDA(cudaSetDevice(c->device));
+  return launch_merge(cand_idx, cand_dist, n, T, k, out_idx, out_dist, (cudaStream_t)stream);
+}
+
+}  // extern "C"

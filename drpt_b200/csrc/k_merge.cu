@@ -1,0 +1,129 @@
+// K7 -- cross-tree merge (the std::merge + std::unique of calculate_nns,
+// mdrpt.cpp:179-198, and the one-rank pass-through of communicate_nns,
+// mdrpt.cpp:580-631).  Each point has T lists of its k nearest leaf-mates
+// (one per tree, sorted by (distance, index), the point itself excluded); the
+// result is its k nearest distinct candidates over all trees.  The same
+// neighbour found in several trees carries the same distance bits (the
+// distance is a deterministic function of the two rows), so a duplicate
+// always meets its twin at the same sort position.
+//
+// One warp per point: lane j holds slot j of the running list (k <= 32) or
+// slots j and j+32 (k <= 64).  Candidates are streamed tree by tree; a
+// candidate enters when it beats the current k-th entry and is not already
+// present, and the lanes shift to make room.
+#include "kernels.cuh"
+
+namespace drpt {
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ bool before(float da, int32_t ia, float db, int32_t ib) {
+  return da < db || (da == db && (uint32_t)ia < (uint32_t)ib);
+}
+
+template <int S>  // slots per lane
+__global__ void __launch_bounds__(kThreads) k_merge(const int32_t *__restrict__ ci,
+                                                    const float *__restrict__ cd, int64_t n, int T,
+                                                    int k, int32_t *__restrict__ oi,
+                                                    float *__restrict__ od) {
+  const int lane = threadIdx.x & 31;
+  const int64_t p = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+  if (p >= n) return;  // warp-uniform: a warp owns one point
+  const float inf = __int_as_float(0x7f800000);
+  float d[S];
+  int32_t id[S];
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    d[s] = inf;
+    id[s] = -1;  // -1 sorts after every index (compared as unsigned)
+  }
+  const int wl = (k - 1) & 31, ws = (k - 1) >> 5;
+  const int32_t *pi = ci + p * T * k;
+  const float *pd = cd + p * T * k;
+  const int total = T * k;
+  for (int base = 0; base < total; base += 32) {
+    const int e = base + lane;
+    const float my_d = e < total ? __ldg(pd + e) : inf;
+    const int32_t my_i = e < total ? __ldg(pi + e) : -1;
+    const int cnt = min(32, total - base);
+    for (int j = 0; j < cnt; ++j) {
+      const float cdv = __shfl_sync(kFull, my_d, j);
+      const int32_t civ = __shfl_sync(kFull, my_i, j);
+      if (civ < 0) continue;  // empty slot of a short leaf (warp-uniform)
+      float wd = inf;
+      int32_t wi = -1;
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        const float td = __shfl_sync(kFull, d[s], wl);
+        const int32_t ti = __shfl_sync(kFull, id[s], wl);
+        if (s == ws) {
+          wd = td;
+          wi = ti;
+        }
+      }
+      if (!before(cdv, civ, wd, wi)) continue;  // not better than the k-th entry
+      bool dup = false;
+      int pos = 0;
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        const bool live = s * 32 + lane < k;
+        dup |= live && id[s] == civ;
+        pos += __popc(__ballot_sync(kFull, live && before(d[s], id[s], cdv, civ)));
+      }
+      if (__any_sync(kFull, dup)) continue;
+      // slot pos takes the candidate, later slots take their predecessor
+      float prev_d = inf;
+      int32_t prev_i = -1;
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        float up_d = __shfl_up_sync(kFull, d[s], 1);
+        int32_t up_i = __shfl_up_sync(kFull, id[s], 1);
+        const float last_d = __shfl_sync(kFull, d[s], 31);
+        const int32_t last_i = __shfl_sync(kFull, id[s], 31);
+        if (lane == 0) {
+          up_d = prev_d;
+          up_i = prev_i;
+        }
+        prev_d = last_d;
+        prev_i = last_i;
+        const int slot = s * 32 + lane;
+        if (slot == pos) {
+          d[s] = cdv;
+          id[s] = civ;
+        } else if (slot > pos) {
+          d[s] = up_d;
+          id[s] = up_i;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const int slot = s * 32 + lane;
+    if (slot < k) {
+      oi[p * k + slot] = id[s];
+      od[p * k + slot] = d[s];
+    }
+  }
+}
+
+}  // namespace
+
+drpt_status launch_merge(const int32_t *cand_idx, const float *cand_dist, int64_t n, int T, int k,
+                         int32_t *out_idx, float *out_dist, cudaStream_t s) {
+  if (k <= 0 || k > kMaxK) {
+    set_error("merge: k = %d outside [1, %d]", k, kMaxK);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  if (n <= 0) return DRPT_OK;
+  const unsigned grid = (unsigned)ceil_div(n * 32, kThreads);
+  if (k <= 32)
+    k_merge<1><<<grid, kThreads, 0, s>>>(cand_idx, cand_dist, n, T, k, out_idx, out_dist);
+  else
+    k_merge<2><<<grid, kThreads, 0, s>>>(cand_idx, cand_dist, n, T, k, out_idx, out_dist);
+  DRPT_LAUNCH_CHECK();
+  return DRPT_OK;
+}
+
+}  // namespace drpt

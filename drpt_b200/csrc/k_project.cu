@@ -1,0 +1,76 @@
+// K1 -- sparse random projection P = X.B (math_operations.cpp:15-46 through
+// an ordered sgemm).  HBM-bound: each point row is read once, coalesced, into
+// shared memory; each output column is written once, coalesced.
+//
+// Per output element the sum runs over the nonzeros of B's column in
+// ascending k with one rounded multiply and one rounded add per term
+// (__fmul_rn / __fadd_rn, never contracted).  Zero entries of B are skipped:
+// for finite inputs they add +-0 to an accumulator that starts at +0 and so
+// never changes it, which keeps P bit-identical to the sequential sum over
+// all d terms.
+#include "kernels.cuh"
+
+namespace drpt {
+namespace {
+
+constexpr int kThreads = 256;
+
+template <typename T>
+__device__ __forceinline__ float to_f(T v) { return (float)v; }
+
+// Block: `pts` consecutive points; thread pairs (point, column) with the
+// point index fastest so a warp writes 32 consecutive P entries of a column.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_project(const T *__restrict__ X, int64_t n, int d,
+                                                      CscDev csc, float *__restrict__ P, int pts) {
+  extern __shared__ float xs[];  // pts x (d + 1), padded against bank conflicts
+  const int64_t p0 = (int64_t)blockIdx.x * pts;
+  const int np = (int)min64(pts, n - p0);
+  const int ld = d + 1;
+  // Stage the rows: consecutive threads read consecutive elements of a row.
+  const int total = np * d;
+  const T *src = X + p0 * d;
+  for (int e = threadIdx.x; e < total; e += kThreads) {
+    const int r = e / d, c = e - r * d;
+    xs[r * ld + c] = to_f(src[e]);
+  }
+  __syncthreads();
+  const int pairs = np * csc.ncols;
+  for (int q = threadIdx.x; q < pairs; q += kThreads) {
+    const int col = q / np, r = q - col * np;
+    const int e0 = __ldg(csc.colptr + col), e1 = __ldg(csc.colptr + col + 1);
+    const float *x = xs + r * ld;
+    float acc = 0.0f;
+    for (int e = e0; e < e1; ++e) acc = __fadd_rn(acc, __fmul_rn(x[__ldg(csc.row + e)], __ldg(csc.val + e)));
+    P[(int64_t)col * n + p0 + r] = acc;
+  }
+}
+
+}  // namespace
+
+drpt_status launch_project(const void *X, int dtype, int64_t n, int d, const CscDev &csc,
+                           float *P, cudaStream_t s) {
+  if (n <= 0 || csc.ncols <= 0) return DRPT_OK;
+  // About 96 KB of staged rows per block, at least 8 and at most 128 points.
+  int pts = (int)(96 * 1024 / ((d + 1) * (int)sizeof(float)));
+  pts = pts < 8 ? 8 : (pts > 128 ? 128 : pts);
+  const size_t smem = (size_t)pts * (d + 1) * sizeof(float);
+  if (smem > 227 * 1024) {
+    set_error("projection: d = %d too large for one staged row block", d);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  const unsigned grid = (unsigned)ceil_div(n, pts);
+  if (dtype == DRPT_DTYPE_U8) {
+    DRPT_CUDA(cudaFuncSetAttribute(k_project<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    k_project<uint8_t><<<grid, kThreads, smem, s>>>((const uint8_t *)X, n, d, csc, P, pts);
+  } else {
+    DRPT_CUDA(cudaFuncSetAttribute(k_project<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    k_project<float><<<grid, kThreads, smem, s>>>((const float *)X, n, d, csc, P, pts);
+  }
+  DRPT_LAUNCH_CHECK();
+  return DRPT_OK;
+}
+
+}  // namespace drpt

@@ -1,0 +1,226 @@
+"""Python front end of libdrpt_gpu.so.
+
+* ``build_graph`` -- one call for the whole path (drpt_build_graph).
+* ``MDRPT`` -- the reference's orchestrator interface (cpp/src/drpt/algo/
+  mdrpt.hpp:102-110): construct, ``grow_trees`` (projection, global trees,
+  local split) and ``gather_nns`` (leaf brute force and cross-tree merge),
+  driven through the kernel-level C entry points.  Errors the reference
+  raises as std::out_of_range arrive here as DrptError with status
+  DRPT_ERR_DEPTH_OUT_OF_RANGE or DRPT_ERR_EMPTY_LEAF.
+
+PyTorch only supplies device memory and streams.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import DrptError, Stats, check
+
+__all__ = ["build_graph", "MDRPT", "DrptError", "edge_list_lines", "global_depth"]
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _is_cuda_tensor(x) -> bool:
+    try:
+        torch = _torch()
+    except ImportError:
+        return False
+    return isinstance(x, torch.Tensor) and x.is_cuda
+
+
+def _dtype_code(x) -> int:
+    if _is_cuda_tensor(x):
+        torch = _torch()
+        if x.dtype == torch.uint8:
+            return _lib.DTYPE_U8
+        if x.dtype == torch.float32:
+            return _lib.DTYPE_F32
+    else:
+        if x.dtype == np.uint8:
+            return _lib.DTYPE_U8
+        if x.dtype == np.float32:
+            return _lib.DTYPE_F32
+    raise TypeError(f"data must be uint8 or float32, got {x.dtype}")
+
+
+def global_depth(n: int, tree_depth_ratio: float = 0.6, tree_depth: int = 0) -> tuple[int, int]:
+    """(tree_depth, global depth) as main.cpp:141-145 and mdrpt.cpp:52 derive them."""
+    td = tree_depth if tree_depth > 0 else int(math.log2(n) - 2)
+    return td, int(td * tree_depth_ratio)
+
+
+def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
+                tree_depth_ratio: float = 0.6, local_tree_offset: int = 2, tree_depth: int = 0,
+                density: float = 0.0, local_seeds=None, device: int = 0, stream=None,
+                out=None):
+    """k-NN graph of `data` (n x d, uint8 or float32; a NumPy array in host
+    memory or a CUDA tensor).  Returns (idx, dist, stats): idx int32 and dist
+    float32 of shape (n, nn), each point's nn nearest distinct neighbours other
+    than itself over all trees, ordered by (distance, index), -1/+inf padded;
+    device tensors when `data` is one.  `out` = (idx, dist) preallocated
+    outputs of the same kind as `data`."""
+    on_dev = _is_cuda_tensor(data)
+    if not on_dev:
+        data = np.ascontiguousarray(data)
+    else:
+        data = data.contiguous()
+    n, d = int(data.shape[0]), int(data.shape[1])
+    desc = _lib.BuildDesc()
+    desc.n, desc.d, desc.dtype = n, d, _dtype_code(data)
+    desc.ntrees, desc.nn = ntrees, nn
+    desc.tree_depth_ratio, desc.local_tree_offset, desc.tree_depth = tree_depth_ratio, \
+        local_tree_offset, tree_depth
+    desc.density, desc.seed = density, seed & 0xFFFFFFFF
+    seeds_arr = None
+    if local_seeds is not None:
+        seeds_arr = (ctypes.c_uint32 * ntrees)(*[int(s) & 0xFFFFFFFF for s in local_seeds])
+        desc.local_seeds = seeds_arr
+    desc.mode = {"exact": _lib.MODE_EXACT, "fast": _lib.MODE_FAST}[mode]
+    desc.data_on_device = 1 if on_dev else 0
+    desc.out_on_device = desc.data_on_device
+    if on_dev:
+        torch = _torch()
+        if stream is None:
+            stream = torch.cuda.current_stream(data.device).cuda_stream
+        device = data.device.index if data.device.index is not None else 0
+        if out is None:
+            idx = torch.empty((n, nn), dtype=torch.int32, device=data.device)
+            dist = torch.empty((n, nn), dtype=torch.float32, device=data.device)
+        else:
+            idx, dist = out
+        ptr_data, ptr_idx, ptr_dist = data.data_ptr(), idx.data_ptr(), dist.data_ptr()
+    else:
+        if out is None:
+            idx = np.empty((n, nn), np.int32)
+            dist = np.empty((n, nn), np.float32)
+        else:
+            idx, dist = out
+        ptr_data, ptr_idx, ptr_dist = data.ctypes.data, idx.ctypes.data, dist.ctypes.data
+    desc.stream = stream or 0
+    ctx = _lib.context(device)
+    stats = Stats()
+    check(_lib.load().drpt_build_graph(ctx.handle, ctypes.byref(desc), ptr_data, ptr_idx, ptr_dist,
+                                       ctypes.byref(stats)))
+    return idx, dist, stats
+
+
+def edge_list_lines(idx: np.ndarray, nn: int) -> list[str]:
+    """The reference's edge-list text (file_writer.cpp:95-149): for every
+    source in ascending order, its first `nn` neighbours as 1-based
+    "src dst" lines.  The reference CLI passes nn-1 (main.cpp:228)."""
+    lines = []
+    for p in range(idx.shape[0]):
+        for q in idx[p, :nn]:
+            if q < 0:
+                break
+            lines.append(f"{p + 1} {int(q) + 1}")
+    return lines
+
+
+class MDRPT:
+    """The reference's MDRPT interface on one GPU (rank 0 of 1).
+
+    Arguments keep the reference's names and meaning (mdrpt.hpp:102-105);
+    `seed` and `local_seeds` replace the std::random_device draws of
+    receive_random_seeds (mdrpt.cpp:402-416).  Data live on `device`."""
+
+    def __init__(self, ntrees: int, tree_depth: int, tree_depth_ratio: float,
+                 local_tree_offset: int, total_data_set_size: int, local_data_set_size: int,
+                 dimension: int, rank: int = 0, world_size: int = 1, input_path: str = "",
+                 output_path: str = "", *, seed: int = 0, local_seeds=None, exact: bool = True,
+                 device: int = 0):
+        if world_size != 1 or rank != 0:
+            raise DrptError(1, "one GPU process: world_size must be 1")
+        self.ntrees, self.tree_depth, self.tree_depth_ratio = ntrees, tree_depth, tree_depth_ratio
+        self.local_tree_offset = local_tree_offset
+        self.n, self.d = int(local_data_set_size), int(dimension)
+        if total_data_set_size != local_data_set_size:
+            raise DrptError(1, "one rank holds every point")
+        self.seed, self.local_seeds = seed & 0xFFFFFFFF, local_seeds
+        self.exact, self.device = exact, device
+        self.input_path, self.output_path = input_path, output_path
+        self._ctx = _lib.context(device)
+        self._L = _lib.load()
+
+    def _stream(self):
+        return _torch().cuda.current_stream(self.device).cuda_stream
+
+    def grow_trees(self, original_data, density: float, use_locality_optimization: bool, nn: int):
+        """Projection, global trees and positional local split
+        (mdrpt.cpp:46-121).  At one rank the locality optimisation only
+        relabels leaves and leaves the graph unchanged; it is accepted and
+        has no effect here."""
+        torch = _torch()
+        dev = torch.device("cuda", self.device)
+        X = original_data if _is_cuda_tensor(original_data) else \
+            torch.from_numpy(np.ascontiguousarray(original_data)).to(dev)
+        X = X.contiguous()
+        self.X, self.dtype_code = X, _dtype_code(X)
+        n, d, T = self.n, self.d, self.ntrees
+        gd = int(self.tree_depth * self.tree_depth_ratio)
+        if gd <= 0 or gd > math.log2(n):
+            raise DrptError(2, f"global depth {gd} outside [1, log2({n})]")
+        self.gd = gd
+        density = density if density else 1.0 / math.sqrt(d)
+        L = gd * T
+        B = np.empty((d, L), np.float32)
+        check(self._L.drpt_host_projection(self.seed, d, L, ctypes.c_float(density),
+                                           B.ctypes.data))
+        self.B = B
+        s = self._stream()
+        cols = np.array([t * gd + lv for t in range(T) for lv in range(gd - 1)], np.int32)
+        P = torch.empty((max(len(cols), 1), n), dtype=torch.float32, device=dev)
+        if len(cols):
+            check(self._L.drpt_project(self._ctx.handle, X.data_ptr(), n, d, self.dtype_code,
+                                       B.ctypes.data, L, cols.ctypes.data, len(cols),
+                                       P.data_ptr(), s))
+        nleaf = 1 << (gd - 1)
+        order = torch.empty((T, n), dtype=torch.int32, device=dev)
+        offs = torch.empty((T, nleaf + 1), dtype=torch.int32, device=dev)
+        med = torch.empty((T, max(nleaf - 1, 1)), dtype=torch.float32, device=dev)
+        check(self._L.drpt_global_trees(self._ctx.handle, P.data_ptr(), n, T, gd,
+                                        1 if self.exact else 0, order.data_ptr(), offs.data_ptr(),
+                                        med.data_ptr(), s))
+        self.P, self.global_order, self.global_offsets, self.medians = P, order, offs, med
+        sizes = (offs[:, 1:] - offs[:, :-1]).cpu().numpy()
+        nonempty = sizes[sizes > 0]
+        min_leaf = int(nonempty.min())
+        ld = int(math.log2(min_leaf) - (math.log2(nn) + self.local_tree_offset))
+        if ld <= 0:
+            raise DrptError(2, f"local tree depth {ld} <= 0")
+        if (sizes == 0).any():
+            raise DrptError(3, "a global leaf is empty")
+        self.ld = ld
+        n_final = nleaf << ld
+        forder = torch.empty((T, n), dtype=torch.int32, device=dev)
+        foffs = torch.empty((T, n_final + 1), dtype=torch.int32, device=dev)
+        check(self._L.drpt_local_leaves(self._ctx.handle, order.data_ptr(), offs.data_ptr(), n, T,
+                                        gd, ld, forder.data_ptr(), foffs.data_ptr(), s))
+        self.final_order, self.final_offsets, self.n_final = forder, foffs, n_final
+
+    def gather_nns(self, nn: int):
+        """Leaf brute force and merge (mdrpt.cpp:273-291).  Returns device
+        tensors (idx, dist) of shape (n, nn)."""
+        torch = _torch()
+        dev = torch.device("cuda", self.device)
+        n, T = self.n, self.ntrees
+        s = self._stream()
+        cidx = torch.empty((n, T, nn), dtype=torch.int32, device=dev)
+        cdist = torch.empty((n, T, nn), dtype=torch.float32, device=dev)
+        check(self._L.drpt_leaf_knn(self._ctx.handle, self.X.data_ptr(), self.dtype_code, n, self.d,
+                                    T, self.final_order.data_ptr(), self.final_offsets.data_ptr(),
+                                    self.n_final, nn, cidx.data_ptr(), cdist.data_ptr(), s))
+        idx = torch.empty((n, nn), dtype=torch.int32, device=dev)
+        dist = torch.empty((n, nn), dtype=torch.float32, device=dev)
+        check(self._L.drpt_merge_candidates(self._ctx.handle, cidx.data_ptr(), cdist.data_ptr(), n,
+                                            T, nn, idx.data_ptr(), dist.data_ptr(), s))
+        self.cand_idx, self.cand_dist = cidx, cdist
+        return idx, dist

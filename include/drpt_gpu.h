@@ -1,0 +1,167 @@
+/*
+ * drpt_gpu.h -- C ABI of libdrpt_gpu.so, the B200 (sm_100a) k-NN-graph path
+ * of DRPT (sparse random projection trees).
+ *
+ * Plain pointers and sizes only; no C++ or framework types cross this
+ * boundary.  Every call returns a drpt_status and never exits or throws;
+ * drpt_last_error() describes the last failure on the calling thread.
+ *
+ * Reference interface each entry point replaces (paths relative to the
+ * reference project root):
+ *   drpt_build_graph      MDRPT::MDRPT + MDRPT::grow_trees + MDRPT::gather_nns
+ *                         (cpp/src/drpt/algo/mdrpt.hpp:102-110, called from
+ *                         cpp/src/main.cpp:198-217); the returned lists feed
+ *                         the edge-list writer (main.cpp:227-228).
+ *   drpt_host_projection  MathOp::build_sparse_projection_matrix
+ *                         (cpp/src/drpt/math/math_operations.hpp:24-26).
+ *   drpt_project          MathOp::multiply_mat (math_operations.hpp:20-21).
+ *   drpt_global_trees     DRPTGlobal::grow_global_tree
+ *                         (cpp/src/drpt/algo/drpt_global.hpp:59-62).
+ *   drpt_local_leaves     MDRPT::grow_local_trees + DRPTLocal
+ *                         (mdrpt.hpp:61-62, drpt_local.hpp:58-69).
+ *   drpt_leaf_knn         MDRPT::calculate_nns (mdrpt.hpp:54-55).
+ *   drpt_merge_candidates the cross-tree merge of calculate_nns /
+ *                         communicate_nns at one rank (mdrpt.hpp:50-52).
+ */
+#ifndef DRPT_GPU_H
+#define DRPT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  DRPT_OK = 0,
+  DRPT_ERR_INVALID_ARG = 1,         /* bad descriptor field or pointer */
+  DRPT_ERR_DEPTH_OUT_OF_RANGE = 2,  /* the reference throws std::out_of_range
+                                       (drpt_global.cpp:155-163,
+                                       drpt_local.cpp:84-92) */
+  DRPT_ERR_EMPTY_LEAF = 3,          /* a global leaf is empty; the reference
+                                       throws from DRPTLocal (log2(0)) */
+  DRPT_ERR_LOCAL_MATRIX_NONZERO = 4,/* exact mode only: a local projection
+                                       matrix is not all zero, so the
+                                       positional local split does not hold */
+  DRPT_ERR_OOM = 5,
+  DRPT_ERR_CUDA = 6,
+  DRPT_ERR_TIMEOUT = 7,             /* a bounded device wait gave up */
+  DRPT_ERR_UNSUPPORTED = 8
+} drpt_status;
+
+typedef enum { DRPT_DTYPE_F32 = 0, DRPT_DTYPE_U8 = 1 } drpt_dtype;
+
+typedef enum {
+  /* Reference-exact plain form: the reference's projection matrix, its
+   * sequential FP32 node statistics and histogram median, its positional
+   * local split and sequential FP32 distances.  Tree assignments are bit-exact
+   * with the reference; neighbour lists match it up to exact-distance ties. */
+  DRPT_MODE_EXACT = 0,
+  /* Plain form with parallel (deterministic, FP64) node statistics; same
+   * algorithm otherwise.  Not bit-exact in tree assignment. */
+  DRPT_MODE_FAST = 1
+} drpt_mode;
+
+typedef struct drpt_ctx drpt_ctx;
+
+typedef struct {
+  int64_t n;                  /* points */
+  int32_t d;                  /* dimensions */
+  int32_t dtype;              /* drpt_dtype of the input rows */
+  int32_t ntrees;             /* -ntrees (main.cpp:61-64) */
+  int32_t nn;                 /* -nn (main.cpp:73-76) */
+  double tree_depth_ratio;    /* -tree-depth-ratio, default 0.6 (main.cpp:35) */
+  int32_t local_tree_offset;  /* -local-tree-offset, default 2 (main.cpp:37) */
+  int32_t tree_depth;         /* 0: int(log2(n) - 2) as main.cpp:141-145 */
+  double density;             /* 0: 1/sqrt(d) (main.cpp:129-132) */
+  uint32_t seed;              /* seed of the global projection matrix */
+  const uint32_t *local_seeds;/* ntrees seeds of the local matrices, or NULL
+                                 (exact mode then skips the all-zero check) */
+  int32_t mode;               /* drpt_mode */
+  int32_t data_on_device;     /* 1: `data` is device memory; 0: host memory */
+  int32_t out_on_device;      /* 1: outputs are device memory; 0: host */
+  void *stream;               /* cudaStream_t to run on; NULL = legacy default */
+} drpt_build_desc;
+
+typedef struct {
+  int32_t tree_depth;         /* total depth before the local split */
+  int32_t global_depth;       /* gd = int(tree_depth * ratio) (mdrpt.cpp:52) */
+  int32_t local_depth;        /* ld (mdrpt.cpp:324) */
+  int32_t n_global_leaves;    /* 2^(gd-1) per tree */
+  int32_t n_final_leaves;     /* 2^(gd-1+ld) per tree */
+  int32_t max_final_leaf;     /* largest final leaf */
+  int64_t min_global_leaf;    /* smallest non-empty global leaf */
+  int64_t sum_leaf_sq;        /* sum over trees and final leaves of m^2 */
+  int32_t kernels_launched;   /* device kernels this call launched */
+  int32_t reserved;
+  float ms_project, ms_global, ms_local, ms_leaf_knn, ms_merge, ms_total;
+} drpt_stats;
+
+/* Library version string. */
+const char *drpt_version(void);
+
+/* Description of the last failure on the calling thread ("" if none). */
+const char *drpt_last_error(void);
+
+/* A context owns the device workspace reused across calls on one device.
+ * One host thread at a time per context. */
+drpt_status drpt_ctx_create(drpt_ctx **ctx, int device);
+void drpt_ctx_destroy(drpt_ctx *ctx);
+
+/* The whole path: projection, global trees, local split, leaf brute force
+ * and cross-tree merge.  `data` is n x d row-major (u8 or f32).  Outputs:
+ * out_idx (int32, n x nn) and out_dist (float, n x nn, may be NULL): for every
+ * point its nn nearest distinct candidates other than itself found in any
+ * tree's final leaf, ordered by (distance, index); missing slots hold -1 and
+ * +inf.  The reference's edge list (file_writer.cpp:36-184, called with
+ * nn-1 at main.cpp:228) is the first nn-1 of them per point. */
+drpt_status drpt_build_graph(drpt_ctx *ctx, const drpt_build_desc *desc, const void *data,
+                             int32_t *out_idx, float *out_dist, drpt_stats *stats);
+
+/* The reference's sparse Gaussian projection matrix on the host, d x L
+ * row-major, from std::mt19937(seed) (math_operations.cpp:48-76). */
+drpt_status drpt_host_projection(uint32_t seed, int32_t d, int32_t L, float density, float *B);
+
+/* Kernel-level entry points (device pointers, stream-ordered on `stream`). */
+
+/* P[c][i] = sum_k X[i][k] * B[k][col(c)] for the listed columns, FP32 in
+ * ascending k without fused multiply-add; P is column-major (ncols x n). */
+drpt_status drpt_project(drpt_ctx *ctx, const void *X, int64_t n, int32_t d, int32_t dtype,
+                         const float *B_host, int32_t L, const int32_t *cols_host,
+                         int32_t ncols, float *P, void *stream);
+
+/* Global trees of all T trees from the projected columns P (column t*(gd-1)
+ * + level, n values each).  order (T x n): point ids grouped by global leaf in
+ * heap order, ascending within a leaf; offsets (T x (2^(gd-1)+1)).  medians
+ * (T x (2^(gd-1)-1), heap numbering) may be NULL.  exact != 0 uses the
+ * reference's sequential FP32 statistics. */
+drpt_status drpt_global_trees(drpt_ctx *ctx, const float *P, int64_t n, int32_t T, int32_t gd,
+                              int32_t exact, int32_t *order, int32_t *offsets, float *medians,
+                              void *stream);
+
+/* Positional local split of every global leaf (offsets as produced above) to
+ * depth ld.  final_order (T x n), final_offsets (T x (2^(gd-1+ld)+1)). */
+drpt_status drpt_local_leaves(drpt_ctx *ctx, const int32_t *order, const int32_t *offsets,
+                              int64_t n, int32_t T, int32_t gd, int32_t ld,
+                              int32_t *final_order, int32_t *final_offsets, void *stream);
+
+/* Exact FP32 brute force inside every final leaf: for each tree and point the
+ * k nearest other members of its leaf by (distance, index).  cand_idx /
+ * cand_dist are n x T x k (point-major). */
+drpt_status drpt_leaf_knn(drpt_ctx *ctx, const void *X, int32_t dtype, int64_t n, int32_t d,
+                          int32_t T, const int32_t *final_order, const int32_t *final_offsets,
+                          int32_t n_final, int32_t k, int32_t *cand_idx, float *cand_dist,
+                          void *stream);
+
+/* Merge of the T per-tree lists of every point into its k nearest distinct
+ * candidates (out_idx / out_dist n x k). */
+drpt_status drpt_merge_candidates(drpt_ctx *ctx, const int32_t *cand_idx, const float *cand_dist,
+                                  int64_t n, int32_t T, int32_t k, int32_t *out_idx,
+                                  float *out_dist, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DRPT_GPU_H */
