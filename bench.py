@@ -1,0 +1,374 @@
+"""Benchmark of the k-NN-graph path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--mode exact|fast] [--impl ours|reference]
+
+Workload (one step = one complete graph build): 1,000,000 x 128 float32
+points, a mixture of 1,000 Gaussian clusters (centres U[0,200]^128, sigma 12,
+clipped to [0,255]), ntrees = 16, nn = 10 -- synthetic data of the shape of
+the fbin workload.  `value` is points/s with the input resident in HBM
+(512 MB, larger than L2, so no flush is needed between steps); `e2e` is the
+same build through the public host-pointer call with the input copied from
+pinned host memory and the neighbour lists copied back, every step.
+
+Under torchrun (N > 1) every rank builds an independent graph of its own
+1M-point dataset (the path has no inter-GPU exchange: replicas, weak
+scaling); the step time is the maximum over ranks.
+
+--impl reference times the reference's own CPU implementation (the reference
+sources built by `make -C oracle ref`, 1 rank x all host threads) on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "kNN-graph points/s at recall@10≥0.90, mixed/learned vs plain FP32, 1 B200"
+N_POINTS, DIM, NTREES, NN, N_CLUSTERS = 1_000_000, 128, 16, 10, 1000
+SEED_PROJ = 12345
+CPU_SAMPLE = 32_768  # bounded sample for the CPU baseline (about 10-30 s of CPU work)
+REF_STEP_SAMPLE = 16_384  # per timed step of --impl reference
+REF_WARMUP_SAMPLE = 4_096  # per untimed warm-up step of --impl reference
+WORKLOAD = ("1,000,000 x 128 float32 (fbin-shaped), 1000 Gaussian clusters, centres U[0,200]^128, "
+            "sigma 12, clipped to [0,255]; ntrees=16, nn=10")
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def _cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[4:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for _, _, r in rows:
+            for nm, v in zip(names, r[1:]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        sm = [r[0] for r in rows]
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(r[1] for r in rows),
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------- reference arm
+def _reference_sample(tmpdir: str, n: int):
+    from drpt_b200 import synth
+    X = synth.clustered_f32(n, DIM, n_clusters=max(1, round(N_CLUSTERS * n / N_POINTS)), seed=2)
+    path = os.path.join(tmpdir, "sample.fbin")
+    synth.write_fbin(path, X)
+    return X, path
+
+
+def run_reference_once(path: str, n: int, threads: int):
+    """One run of the reference binary; returns (build_s, query_s, kind)."""
+    ref = os.path.join(ROOT, "oracle", "_ref", "drpt_ref")
+    seeds = ",".join(str(s) for s in [SEED_PROJ] + list(range(1, NTREES + 1)))
+    if os.path.exists(ref):
+        out_dir = tempfile.mkdtemp()
+        cmd = (f"ulimit -s unlimited; exec {ref} -input {path} -output {out_dir}/ -data-set-size {n} "
+               f"-dimension {DIM} -ntrees {NTREES} -nn {NN} -locality 0 -data-file-format 1 -no-write")
+        env = dict(os.environ, DRPT_REF_SEEDS=seeds, OMP_NUM_THREADS=str(threads),
+                   OMP_PROC_BIND="true")
+        r = subprocess.run(["bash", "-c", cmd], env=env, capture_output=True, text=True)
+        shutil.rmtree(out_dir, ignore_errors=True)
+        m = re.search(r"Index building \(s\)\s*([0-9.eE+-]+)\s*Querying Time \(s\)\s*([0-9.eE+-]+)",
+                      r.stdout)
+        if r.returncode != 0 or not m:
+            raise RuntimeError(f"reference run failed: {r.stderr[-500:]}")
+        return float(m.group(1)), float(m.group(2)), "reference"
+    # The reference tree was not built here: time the CPU restatement instead.
+    import oracle
+    from drpt_b200 import synth
+    X = synth.read_fbin(path)
+    t0 = time.perf_counter()
+    o = oracle.build(X, NTREES, NN, SEED_PROJ)
+    t1 = time.perf_counter()
+    if o["status"] != 0:
+        raise RuntimeError(f"oracle build failed: {o['status']}")
+    return t1 - t0, 0.0, "port"
+
+
+def cpu_baseline(n: int = CPU_SAMPLE):
+    threads = _cores()
+    with tempfile.TemporaryDirectory() as tmp:
+        _, path = _reference_sample(tmp, n)
+        b, q, kind = run_reference_once(path, n, threads)
+    return {"value": n / (b + q), "unit": "points/s", "cores": threads if kind == "reference" else 1,
+            "kind": kind,
+            "sample": f"{n} points of the same distribution (clusters scaled to {max(1, round(N_CLUSTERS * n / N_POINTS))}), "
+                      f"ntrees={NTREES}, nn={NN}, 1 rank x {threads if kind == 'reference' else 1} threads; "
+                      f"time = index building + querying ({b:.2f} s + {q:.2f} s)"}
+
+
+def reference_arm(args):
+    rank = _env_int("RANK", 0)
+    if rank != 0:
+        return
+    threads = _cores()
+    times = []
+    with tempfile.TemporaryDirectory() as tmp:
+        _, wpath = _reference_sample(tmp, REF_WARMUP_SAMPLE)
+        for _ in range(args.warmup):
+            run_reference_once(wpath, REF_WARMUP_SAMPLE, threads)
+        _, path = _reference_sample(tmp, REF_STEP_SAMPLE)
+        kind = "reference"
+        for _ in range(args.steps):
+            b, q, kind = run_reference_once(path, REF_STEP_SAMPLE, threads)
+            times.append(b + q)
+    sec = sum(times) / len(times)
+    value = REF_STEP_SAMPLE / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "points/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_points": REF_STEP_SAMPLE, "ranks": 1,
+                   "threads": threads},
+        "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads if kind == "reference" else 1,
+                         "kind": kind,
+                         "sample": f"{REF_STEP_SAMPLE} points of the same distribution per timed step "
+                                   f"(warm-up steps: {REF_WARMUP_SAMPLE} points)"},
+        "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+def _traffic_per_launch(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        data = json.load(open(path))
+        return data.get(kernel, {}).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--mode", default="exact", choices=["exact", "fast"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from drpt_b200 import build_graph, recall, synth
+
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local_rank = _env_int("LOCAL_RANK", 0)
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+
+    X = synth.clustered_f32(N_POINTS, DIM, n_clusters=N_CLUSTERS, seed=2 + rank)
+    Xd = torch.from_numpy(X).to(dev)
+    idx = torch.empty((N_POINTS, NN), dtype=torch.int32, device=dev)
+    dst = torch.empty((N_POINTS, NN), dtype=torch.float32, device=dev)
+
+    def step():
+        return build_graph(Xd, NTREES, NN, SEED_PROJ + rank, mode=args.mode, out=(idx, dst))[2]
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        st = step()
+    torch.cuda.synchronize()
+
+    # device-resident timing
+    per_kernel = {"leaf_knn": [], "global": [], "project": [], "merge": [], "local": []}
+    launches = 0
+    with ClockSampler(local_rank) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            st = step()
+            per_kernel["leaf_knn"].append(st.ms_leaf_knn)
+            per_kernel["global"].append(st.ms_global)
+            per_kernel["project"].append(st.ms_project)
+            per_kernel["merge"].append(st.ms_merge)
+            per_kernel["local"].append(st.ms_local)
+            launches += st.kernels_launched
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    clk = clocks.summary()
+
+    # end to end through the host-pointer call, pinned buffers
+    e2e = None
+    if not args.no_e2e:
+        Xh = torch.from_numpy(X).pin_memory()
+        oi = torch.empty((N_POINTS, NN), dtype=torch.int32).pin_memory()
+        od = torch.empty((N_POINTS, NN), dtype=torch.float32).pin_memory()
+        xnp, inp, dnp = Xh.numpy(), oi.numpy(), od.numpy()
+        build_graph(xnp, NTREES, NN, SEED_PROJ + rank, mode=args.mode, out=(inp, dnp),
+                    stream=stream.cuda_stream)
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            build_graph(xnp, NTREES, NN, SEED_PROJ + rank, mode=args.mode, out=(inp, dnp),
+                        stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+        if world > 1:
+            t = torch.tensor([e2e_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": world * N_POINTS / (e2e_ms / 1e3), "unit": "points/s",
+               "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(X.nbytes),
+               "d2h_bytes_per_step": int(oi.numel() * 4 + od.numel() * 4)}
+
+    # recall@10 on a seeded sample against FP64 exact neighbours
+    q = recall.sample_queries(N_POINTS, 1000, seed=7)
+    true_i, _ = recall.exact_knn_fp64(Xd, q, NN, device=local_rank)
+    rec = recall.recall_at_k(idx.cpu().numpy()[q], true_i)
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    # roofline of the dominant kernel (leaf brute force), exact FP32 SIMT:
+    # 3 FP32 operations (subtract, multiply, add) per pair and dimension
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    leaf_ms = statistics.median(per_kernel["leaf_knn"])
+    flops = 3.0 * st.sum_leaf_sq * DIM
+    achieved = flops / (leaf_ms * 1e-3) / 1e12
+    sm_mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = 148 * 128 * sm_mhz * 1e6 / 1e12  # one FP32 op per lane per clock (no FMA pairing)
+    traffic = _traffic_per_launch("k_leaf_knn")
+    roofline = {"kernel": "k_leaf_knn (exact FP32 leaf brute force)", "bound": "fp32",
+                "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "traffic": traffic,
+                "peak_source": "nominal FP32 issue rate (148 SMs x 128 lanes x median SM clock); "
+                               "MEASURED_PEAKS.json holds no FP32 figure",
+                "algorithmic_flops_per_launch": flops,
+                "hbm_bytes_alg_per_launch": float(N_POINTS * NTREES * DIM * 4),
+                "hbm_frac_of_measured": (N_POINTS * NTREES * DIM * 4 / (leaf_ms * 1e-3) / 1e9) /
+                                        peaks.get("hbm_gbs", 6651.7)}
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            cpu = cpu_baseline()
+        except Exception as ex:  # reported, not fatal
+            cpu = {"value": None, "unit": "points/s", "error": str(ex)[:200]}
+    line = {
+        "metric": METRIC, "value": world * N_POINTS / (ms / 1e3), "unit": "points/s",
+        "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "mode": args.mode, "recall@10": rec,
+                   "recall_sample": 1000, "global_depth": st.global_depth,
+                   "local_depth": st.local_depth, "mean_leaf": st.sum_leaf_sq / (NTREES * N_POINTS),
+                   "phase_ms": {k: statistics.median(v) for k, v in per_kernel.items()},
+                   "l2": "input 512 MB > 126 MB L2; no flush between steps",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

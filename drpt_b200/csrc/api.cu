@@ -148,24 +148,39 @@ drpt_status global_trees(drpt_ctx *c, const float *P, int64_t n, int T, int gd, 
     *off_out = off[0];
     return DRPT_OK;
   }
+  // level scratch, sized for the deepest level
+  const int last = gd - 2;
+  const int64_t Gmax = (int64_t)T << last;
+  const int64_t Umax = tree_level_max_units(n, T, last);
+  TreeLevelArgs a{};
+  DRPT_TRY(ws_get(c, "lv_node_ubase", Gmax + 1, &a.node_ubase));
+  DRPT_TRY(ws_get(c, "lv_unit_node", Umax, &a.unit_node));
+  DRPT_TRY(ws_get(c, "lv_unit_lo", Umax, &a.unit_lo));
+  DRPT_TRY(ws_get(c, "lv_n_units", 1, &a.n_units));
+  DRPT_TRY(ws_get(c, "lv_node_D", Gmax * kBins, &a.node_D));
+  DRPT_TRY(ws_get(c, "lv_unit_s", 2 * Umax, &a.unit_s));
+  DRPT_TRY(ws_get(c, "lv_unit_hist", Umax * kBins, &a.unit_hist));
+  DRPT_TRY(ws_get(c, "lv_node_med", Gmax, &a.node_med));
+  DRPT_TRY(ws_get(c, "lv_unit_left", Umax, &a.unit_left));
+  DRPT_TRY(ws_get(c, "lv_unit_lbase", Umax, &a.unit_lbase));
+  DRPT_TRY(ws_get(c, "lv_node_nleft", Gmax, &a.node_nleft));
   int cur = 0;
   for (int level = 0; level < gd - 1; ++level) {
-    LevelArgs a;
     a.P = P;
     a.n = n;
     a.T = T;
     a.gd = gd;
     a.level = level;
     a.ord_in = level == 0 ? nullptr : ord[cur];
-    a.val_in = level == 0 ? P : val[cur];
+    a.val_in = level == 0 ? nullptr : val[cur];
     a.off_in = level == 0 ? nullptr : off[cur];
     a.ord_out = ord[cur ^ 1];
     a.val_out = level + 1 < gd - 1 ? val[cur ^ 1] : nullptr;
     a.off_out = off[cur ^ 1];
     a.medians = medians;
     a.exact = exact;
-    DRPT_TRY(launch_level(a, s));
-    c->launches += 1;
+    DRPT_TRY(launch_tree_level(a, tree_level_max_units(n, T, level), s));
+    c->launches += tree_level_kernels(exact);
     cur ^= 1;
   }
   *order_out = ord[cur];
@@ -418,7 +433,7 @@ drpt_status drpt_build_graph(drpt_ctx *c, const drpt_build_desc *desc, const voi
   DRPT_TRY(ws_get(c, "cand_dist", (size_t)n * T * nn, &cdist));
   LeafKnnArgs ka{X, desc->dtype, n, d, T, nn, forder, foff, n_final, cidx, cdist};
   DRPT_TRY(launch_leaf_knn_exact(ka, s));
-  c->launches += 1;
+  c->launches += leaf_knn_exact_kernels();
   DRPT_CUDA(cudaEventRecord(ev[4], s));
 
   // K7: merge into the output.

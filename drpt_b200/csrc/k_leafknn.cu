@@ -3,14 +3,19 @@
 // 385-396).
 //
 // One thread block per (tree, final leaf).  The leaf's rows are gathered from
-// X in chunks of 32 dimensions into shared memory; 256 threads each own a 4x4
-// block of (row, column) pairs of a 64x64 tile and keep the distance chains
-// in registers:  acc = acc + (q_i - p_i)^2 for i ascending, each subtract,
+// X in chunks of 32 dimensions into shared memory (zero-padded past d); 256
+// threads on a 16 x 16 grid each own an MT x MT block of (row, column) pairs
+// of a TM x TM tile (TM = 16 * MT) and keep the distance chains in
+// registers:  acc = acc + (q_i - p_i)^2 for i ascending, each subtract,
 // multiply and add rounded on its own, then sqrt -- the reference's saxpy
 // (-1) + snrm2 sequence, so every distance is bit-identical to the
-// reference's.  One thread per row then folds the tile's 64 candidates into
-// the row's running k nearest by (distance, index), skipping the point
-// itself.  Leaves larger than 64 loop over 64x64 tiles.
+// reference's (a zero-padded dimension adds (0 - 0)^2 = +0, which leaves a
+// non-negative sum unchanged).  One thread per row then folds the tile's
+// candidates into the row's running k nearest by (distance, index), skipping
+// the point itself.  Two instantiations: TM = 64 serves leaves of up to 64
+// points and those above 128 (looping over 64 x 64 tiles), TM = 128 the
+// leaves of 65 to 128 points in one tile; each launch covers every leaf and
+// returns at once for the other class.
 //
 // Output: for point p and tree t, cand[(p*T + t)*k + j], j < k, sorted; slots
 // beyond the leaf size hold index -1 and distance +inf.
@@ -20,73 +25,84 @@ namespace drpt {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kTile = 64;
 constexpr int kChunk = 32;             // dimensions staged per step
 constexpr int kLd = kChunk + 1;        // padded row stride in shared memory
 
-template <typename T>
+template <int TM, typename T>
 __device__ __forceinline__ void stage_rows(float *dst, const T *__restrict__ X, int d,
-                                           const int32_t *ids, int rows, int k0, int kc) {
-  for (int e = threadIdx.x; e < kTile * kChunk; e += kThreads) {
+                                           const int32_t *ids, int rows, int k0) {
+  for (int e = threadIdx.x; e < TM * kChunk; e += kThreads) {
     const int r = e / kChunk, kk = e - r * kChunk;
     float v = 0.0f;
-    if (r < rows && kk < kc) v = (float)X[(int64_t)ids[r] * d + k0 + kk];
+    if (r < rows && k0 + kk < d) v = (float)X[(int64_t)ids[r] * d + k0 + kk];
     dst[r * kLd + kk] = v;
   }
 }
 
-template <typename T>
+template <int TM>
+constexpr size_t leaf_smem(int k) {
+  return sizeof(float) * (2 * TM * kLd + TM * (TM + 1)) +
+         (sizeof(float) + sizeof(int32_t)) * TM * (k + 1) + sizeof(int32_t) * 2 * TM;
+}
+
+template <int TM, typename T>
 __global__ void __launch_bounds__(kThreads) k_leaf_knn(LeafKnnArgs a) {
+  constexpr int MT = TM / 16;
+  // TM = 128 serves 64 < m <= 128 (one tile); TM = 64 serves m <= 64 and,
+  // with less padding than 128-wide tiles, every leaf above 128.
   extern __shared__ float smem[];
-  float *xr = smem;                          // kTile x kLd
-  float *xc = xr + kTile * kLd;              // kTile x kLd
-  float *dt = xc + kTile * kLd;              // kTile x (kTile + 1)
-  float *topd = dt + kTile * (kTile + 1);    // kTile x (k + 1)
-  int32_t *topi = (int32_t *)(topd + kTile * (a.k + 1));
-  int32_t *rid = topi + kTile * (a.k + 1);   // kTile
-  int32_t *cid = rid + kTile;                // kTile
+  float *xr = smem;                          // TM x kLd
+  float *xc = xr + TM * kLd;                 // TM x kLd
+  float *dt = xc + TM * kLd;                 // TM x (TM + 1)
+  float *topd = dt + TM * (TM + 1);          // TM x (k + 1)
+  int32_t *topi = (int32_t *)(topd + TM * (a.k + 1));
+  int32_t *rid = topi + TM * (a.k + 1);      // TM
+  int32_t *cid = rid + TM;                   // TM
 
   const int t = blockIdx.x / a.n_final, f = blockIdx.x - t * a.n_final;
   const int32_t *off = a.final_off + (int64_t)t * (a.n_final + 1);
   const int32_t b = off[f], m = off[f + 1] - b;
+  const bool mine = TM == 128 ? (m > 64 && m <= 128) : (m <= 64 || m > 128);
+  if (!mine) return;
   const int32_t *members = a.final_order + (int64_t)t * a.n + b;
   const T *X = (const T *)a.X;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int kp1 = a.k + 1;
+  const float inf = __int_as_float(0x7f800000);
 
-  for (int r0 = 0; r0 < m; r0 += kTile) {
-    const int rows = min(kTile, m - r0);
-    for (int i = threadIdx.x; i < kTile * kp1; i += kThreads) {
-      topd[i] = __int_as_float(0x7f800000);  // +inf
+  for (int r0 = 0; r0 < m; r0 += TM) {
+    const int rows = min(TM, m - r0);
+    for (int i = threadIdx.x; i < TM * kp1; i += kThreads) {
+      topd[i] = inf;
       topi[i] = INT32_MAX;
     }
-    if (threadIdx.x < kTile) rid[threadIdx.x] = threadIdx.x < rows ? members[r0 + threadIdx.x] : -1;
-    for (int c0 = 0; c0 < m; c0 += kTile) {
-      const int cols = min(kTile, m - c0);
+    if (threadIdx.x < TM) rid[threadIdx.x] = threadIdx.x < rows ? members[r0 + threadIdx.x] : -1;
+    for (int c0 = 0; c0 < m; c0 += TM) {
+      const int cols = min(TM, m - c0);
       const bool same = (c0 == r0);
-      if (threadIdx.x < kTile) cid[threadIdx.x] = threadIdx.x < cols ? members[c0 + threadIdx.x] : -1;
+      if (threadIdx.x < TM) cid[threadIdx.x] = threadIdx.x < cols ? members[c0 + threadIdx.x] : -1;
       __syncthreads();
-      float acc[4][4];
+      float acc[MT][MT];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < MT; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+        for (int j = 0; j < MT; ++j) acc[i][j] = 0.0f;
       const float *xcol = same ? xr : xc;
       for (int k0 = 0; k0 < a.d; k0 += kChunk) {
-        const int kc = min(kChunk, a.d - k0);
-        stage_rows(xr, X, a.d, rid, rows, k0, kc);
-        if (!same) stage_rows(xc, X, a.d, cid, cols, k0, kc);
+        stage_rows<TM>(xr, X, a.d, rid, rows, k0);
+        if (!same) stage_rows<TM>(xc, X, a.d, cid, cols, k0);
         __syncthreads();
-        for (int kk = 0; kk < kc; ++kk) {
-          float av[4], bv[4];
+#pragma unroll 4
+        for (int kk = 0; kk < kChunk; ++kk) {
+          float av[MT], bv[MT];
 #pragma unroll
-          for (int i = 0; i < 4; ++i) av[i] = xr[(ty + 16 * i) * kLd + kk];
+          for (int i = 0; i < MT; ++i) av[i] = xr[(ty + 16 * i) * kLd + kk];
 #pragma unroll
-          for (int j = 0; j < 4; ++j) bv[j] = xcol[(tx + 16 * j) * kLd + kk];
+          for (int j = 0; j < MT; ++j) bv[j] = xcol[(tx + 16 * j) * kLd + kk];
 #pragma unroll
-          for (int i = 0; i < 4; ++i)
+          for (int i = 0; i < MT; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
+            for (int j = 0; j < MT; ++j) {
               const float df = __fsub_rn(bv[j], av[i]);
               acc[i][j] = __fadd_rn(acc[i][j], __fmul_rn(df, df));
             }
@@ -94,21 +110,21 @@ __global__ void __launch_bounds__(kThreads) k_leaf_knn(LeafKnnArgs a) {
         __syncthreads();
       }
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < MT; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) dt[(ty + 16 * i) * (kTile + 1) + tx + 16 * j] = __fsqrt_rn(acc[i][j]);
+        for (int j = 0; j < MT; ++j) dt[(ty + 16 * i) * (TM + 1) + tx + 16 * j] = __fsqrt_rn(acc[i][j]);
       __syncthreads();
       if (threadIdx.x < rows) {
         const int r = threadIdx.x;
         const int32_t p = rid[r];
         float *ld = topd + r * kp1;
         int32_t *li = topi + r * kp1;
+        float wd = ld[a.k - 1];
+        int32_t wi = li[a.k - 1];
         for (int c = 0; c < cols; ++c) {
           const int32_t q = cid[c];
-          if (q == p) continue;
-          const float dv = dt[r * (kTile + 1) + c];
-          const float wd = ld[a.k - 1];
-          if (!(dv < wd || (dv == wd && q < li[a.k - 1]))) continue;
+          const float dv = dt[r * (TM + 1) + c];
+          if (q == p || !(dv < wd || (dv == wd && q < wi))) continue;
           int j = a.k - 1;
           while (j > 0 && (dv < ld[j - 1] || (dv == ld[j - 1] && q < li[j - 1]))) {
             ld[j] = ld[j - 1];
@@ -117,6 +133,8 @@ __global__ void __launch_bounds__(kThreads) k_leaf_knn(LeafKnnArgs a) {
           }
           ld[j] = dv;
           li[j] = q;
+          wd = ld[a.k - 1];
+          wi = li[a.k - 1];
         }
       }
       __syncthreads();
@@ -127,11 +145,21 @@ __global__ void __launch_bounds__(kThreads) k_leaf_knn(LeafKnnArgs a) {
       for (int j = 0; j < a.k; ++j) {
         const bool have = topi[r * kp1 + j] != INT32_MAX;
         a.cand_idx[o + j] = have ? topi[r * kp1 + j] : -1;
-        a.cand_dist[o + j] = have ? topd[r * kp1 + j] : __int_as_float(0x7f800000);
+        a.cand_dist[o + j] = have ? topd[r * kp1 + j] : inf;
       }
     }
     __syncthreads();
   }
+}
+
+template <int TM, typename T>
+drpt_status launch_one(const LeafKnnArgs &a, unsigned blocks, cudaStream_t s) {
+  const size_t smem = leaf_smem<TM>(a.k);
+  DRPT_CUDA(cudaFuncSetAttribute(k_leaf_knn<TM, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  k_leaf_knn<TM, T><<<blocks, kThreads, smem, s>>>(a);
+  DRPT_LAUNCH_CHECK();
+  return DRPT_OK;
 }
 
 }  // namespace
@@ -143,19 +171,17 @@ drpt_status launch_leaf_knn_exact(const LeafKnnArgs &a, cudaStream_t s) {
   }
   const int64_t blocks = (int64_t)a.T * a.n_final;
   if (blocks <= 0) return DRPT_OK;
-  const size_t smem = sizeof(float) * (2 * kTile * kLd + kTile * (kTile + 1)) +
-                      (sizeof(float) + sizeof(int32_t)) * kTile * (a.k + 1) + sizeof(int32_t) * 2 * kTile;
+  if (blocks > 0x7fffffff) return DRPT_ERR_UNSUPPORTED;
   if (a.dtype == DRPT_DTYPE_U8) {
-    DRPT_CUDA(cudaFuncSetAttribute(k_leaf_knn<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
-    k_leaf_knn<uint8_t><<<(unsigned)blocks, kThreads, smem, s>>>(a);
+    DRPT_TRY((launch_one<64, uint8_t>(a, (unsigned)blocks, s)));
+    DRPT_TRY((launch_one<128, uint8_t>(a, (unsigned)blocks, s)));
   } else {
-    DRPT_CUDA(cudaFuncSetAttribute(k_leaf_knn<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
-    k_leaf_knn<float><<<(unsigned)blocks, kThreads, smem, s>>>(a);
+    DRPT_TRY((launch_one<64, float>(a, (unsigned)blocks, s)));
+    DRPT_TRY((launch_one<128, float>(a, (unsigned)blocks, s)));
   }
-  DRPT_LAUNCH_CHECK();
   return DRPT_OK;
 }
+
+int leaf_knn_exact_kernels() { return 2; }
 
 }  // namespace drpt

@@ -39,18 +39,32 @@ __global__ void __launch_bounds__(kThreads) k_merge(const int32_t *__restrict__ 
     id[s] = -1;  // -1 sorts after every index (compared as unsigned)
   }
   const int wl = (k - 1) & 31, ws = (k - 1) >> 5;
-  const int32_t *pi = ci + p * T * k;
-  const float *pd = cd + p * T * k;
-  const int total = T * k;
-  for (int base = 0; base < total; base += 32) {
-    const int e = base + lane;
-    const float my_d = e < total ? __ldg(pd + e) : inf;
-    const int32_t my_i = e < total ? __ldg(pi + e) : -1;
-    const int cnt = min(32, total - base);
-    for (int j = 0; j < cnt; ++j) {
-      const float cdv = __shfl_sync(kFull, my_d, j);
-      const int32_t civ = __shfl_sync(kFull, my_i, j);
-      if (civ < 0) continue;  // empty slot of a short leaf (warp-uniform)
+  // Tree by tree: each list is sorted, so once an entry fails to beat the
+  // current k-th, the rest of that list cannot enter either.
+  for (int t = 0; t < T; ++t) {
+    const int32_t *pi = ci + (p * T + t) * k;
+    const float *pd = cd + (p * T + t) * k;
+    float ld[S];
+    int32_t li[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      const int e = s * 32 + lane;
+      ld[s] = e < k ? __ldg(pd + e) : inf;
+      li[s] = e < k ? __ldg(pi + e) : -1;
+    }
+    for (int j = 0; j < k; ++j) {
+      float cdv = inf;
+      int32_t civ = -1;
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        const float td = __shfl_sync(kFull, ld[s], j & 31);
+        const int32_t ti = __shfl_sync(kFull, li[s], j & 31);
+        if (s == (j >> 5)) {
+          cdv = td;
+          civ = ti;
+        }
+      }
+      if (civ < 0) break;  // the rest of this list is empty (warp-uniform)
       float wd = inf;
       int32_t wi = -1;
 #pragma unroll
@@ -62,7 +76,7 @@ __global__ void __launch_bounds__(kThreads) k_merge(const int32_t *__restrict__ 
           wi = ti;
         }
       }
-      if (!before(cdv, civ, wd, wi)) continue;  // not better than the k-th entry
+      if (!before(cdv, civ, wd, wi)) break;  // not better than the k-th entry
       bool dup = false;
       int pos = 0;
 #pragma unroll

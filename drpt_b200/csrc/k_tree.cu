@@ -3,19 +3,31 @@
 // MathOp::distributed_mean/_variance/_median, math_operations.cpp:121-383, at
 // one rank).
 //
-// One thread block per (tree, node).  A node's points are a contiguous range
-// of the tree's `ord` array in ascending point index, because the partition
-// below is stable and the root starts in index order; their split values are
-// the matching range of `val`.
+// A node's points are a contiguous range of the tree's `ord` array in
+// ascending point index (the root starts in index order and every partition
+// is stable); `val` holds the matching split values.  The work of a level is
+// cut into units of up to kUnit consecutive positions that never straddle a
+// node, so large nodes near the root spread over the whole GPU and small
+// nodes near the leaves cost one unit each:
 //
-// exact = 1 reproduces the reference bit for bit: the mean and the squared
-// deviations are summed one value at a time in list order in FP32 (a single
-// dependent add chain per node, run by warp 0; the warp loads 256 values per
-// step coalesced and broadcasts them with shuffles), and every float or
-// double operation of the boundaries and of the median interpolation rounds
-// on its own (__f*_rn / __d*_rn).
-// exact = 0 sums in FP64 with a fixed block-wide reduction order (the same
-// result on every run, not the reference's).
+//   plan      one block: units per node, their prefix, unit -> (node, start)
+//   stats     exact: one block per node runs the reference's sequential FP32
+//             sums (a single dependent add chain: warp 0 adds the values in
+//             list order from a shared-memory double buffer that the other
+//             warps fill); fast: FP64 partial sums per unit, combined per
+//             node in unit order
+//   bounds    16 histogram boundaries per node (exact float arithmetic)
+//   hist      per unit, 16 integer counts
+//   median    per node: counts summed in unit order, selection and the
+//             double-precision interpolation of the reference
+//   count     per unit, values <= median
+//   scan      per node: unit prefix of the left counts, child offsets
+//   scatter   per unit: stable partition through shared memory, coalesced
+//             writes of the point ids and of their next-level values
+//
+// Every operation that the reference performs in float or double rounds on
+// its own here (__f*_rn / __d*_rn), so with exact = 1 the medians, and hence
+// the trees, are bit-identical to the reference's.
 #include "kernels.cuh"
 
 namespace drpt {
@@ -23,89 +35,11 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+constexpr int kUnit = 4096;                  // positions per unit
+constexpr int kPer = kUnit / kThreads;       // positions per thread in a unit
+constexpr int kChainChunk = 2048;            // values per shared-memory buffer of the chain
 
-// Dependent FP32 chain over v[0..n): s = s + f(v[i]) in index order, where
-// f is the identity or (v - mu)^2 with a rounded subtract and multiply.
-// Called by one full warp; every lane returns the sum.
-template <bool kSq>
-__device__ float warp_chain(const float *__restrict__ v, int64_t n, float mu) {
-  const int lane = threadIdx.x & 31;
-  constexpr int U = 8;
-  constexpr int STEP = 32 * U;
-  const int64_t full = (n / STEP) * STEP;
-  float s = 0.0f;
-  float cur[U], nxt[U];
-#pragma unroll
-  for (int u = 0; u < U; ++u) cur[u] = full > 0 ? __ldg(v + u * 32 + lane) : 0.0f;
-  for (int64_t b = 0; b < full; b += STEP) {
-    const int64_t nb = b + STEP;
-#pragma unroll
-    for (int u = 0; u < U; ++u) nxt[u] = nb < full ? __ldg(v + nb + u * 32 + lane) : 0.0f;
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      float x = cur[u];
-      if (kSq) {
-        const float df = __fsub_rn(x, mu);
-        x = __fmul_rn(df, df);
-      }
-#pragma unroll
-      for (int j = 0; j < 32; ++j) s = __fadd_rn(s, __shfl_sync(kFull, x, j));
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) cur[u] = nxt[u];
-  }
-  for (int64_t b = full; b < n; b += 32) {
-    float x = (b + lane < n) ? __ldg(v + b + lane) : 0.0f;
-    if (kSq) {
-      const float df = __fsub_rn(x, mu);
-      x = __fmul_rn(df, df);
-    }
-    const int cnt = (int)min64(32, n - b);
-    for (int j = 0; j < cnt; ++j) s = __fadd_rn(s, __shfl_sync(kFull, x, j));
-  }
-  return s;
-}
-
-// Fixed-order block reduction of two doubles; result valid in all threads.
-__device__ void block_sum2(double &a, double &b, double *sh) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_down_sync(kFull, a, o);
-    b += __shfl_down_sync(kFull, b, o);
-  }
-  if (lane == 0) {
-    sh[2 * w] = a;
-    sh[2 * w + 1] = b;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double ta = 0.0, tb = 0.0;
-    for (int i = 0; i < kWarps; ++i) {
-      ta += sh[2 * i];
-      tb += sh[2 * i + 1];
-    }
-    sh[2 * kWarps] = ta;
-    sh[2 * kWarps + 1] = tb;
-  }
-  __syncthreads();
-  a = sh[2 * kWarps];
-  b = sh[2 * kWarps + 1];
-  __syncthreads();
-}
-
-__device__ int block_count(int c, int *sh) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
-  if (lane == 0) sh[w] = c;
-  __syncthreads();
-  int tot = 0;
-  for (int i = 0; i < kWarps; ++i) tot += sh[i];
-  __syncthreads();
-  return tot;
-}
-
+// ------------------------------------------------------------------ helpers
 // Histogram boundaries (math_operations.cpp:252-288, factor 1, 7 bins):
 // slots 0..13 around the mean at multiples of sigma/30, sigma/6 and sigma/2;
 // slots 14 and 15 stay 0.
@@ -133,7 +67,8 @@ __device__ void node_bounds(float mu, float sigma, float *D) {
 }
 
 // Slot of x (math_operations.cpp:292-308): slot j in 1..15 when
-// D[j-1] < x <= D[j]; slot 0 when no slot takes it.
+// D[j-1] < x <= D[j]; slot 0 when no slot takes it.  D[0..13] never
+// decrease and (D[13], 0] cannot overlap them, so at most one j matches.
 __device__ __forceinline__ int bin_of(const float *D, float x) {
   int slot = 0;
 #pragma unroll
@@ -165,142 +100,396 @@ __device__ float node_median(const float *D, const unsigned *hist, int64_t n) {
   return __double2float_rn(__dadd_rn((double)lo, __dmul_rn(frac, (double)width)));
 }
 
-__global__ void __launch_bounds__(kThreads) k_level(LevelArgs a, int64_t val_stride) {
-  __shared__ float sD[kBins];
-  __shared__ unsigned sHist[kWarps][kBins];
-  __shared__ float sStat[2];
-  __shared__ double sRed[2 * kWarps + 2];
-  __shared__ int sCnt[kWarps];
-  __shared__ int sScan[kWarps + 1];
+struct NodeRange {
+  int64_t lo, hi;
+};
 
+__device__ __forceinline__ NodeRange node_range(const TreeLevelArgs &a, int g) {
   const int nodes = 1 << a.level;
-  const int t = blockIdx.x / nodes, node = blockIdx.x - t * nodes;
-  const int64_t lo = a.off_in ? a.off_in[(int64_t)t * (nodes + 1) + node] : 0;
-  const int64_t hi = a.off_in ? a.off_in[(int64_t)t * (nodes + 1) + node + 1] : a.n;
-  const int64_t cnt = hi - lo;
-  const float *v = a.val_in + (int64_t)t * val_stride + lo;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int t = g >> a.level, s = g & (nodes - 1);
+  if (!a.off_in) return {0, a.n};
+  const int32_t *o = a.off_in + (int64_t)t * (nodes + 1);
+  return {o[s], o[s + 1]};
+}
 
-  // 1. mean and variance
-  if (a.exact) {
-    if (warp == 0) {
-      const float sum = warp_chain<false>(v, cnt, 0.0f);
-      const float mu = __fdiv_rn(sum, __int2float_rn((int)cnt));
-      const float sq = warp_chain<true>(v, cnt, mu);
-      const float var = __fdiv_rn(sq, __int2float_rn((int)cnt - 1));
-      if (lane == 0) {
-        sStat[0] = mu;
-        sStat[1] = var;
-      }
-    }
-  } else {
-    double s1 = 0.0, s2 = 0.0;
-    for (int64_t i = threadIdx.x; i < cnt; i += kThreads) {
-      const double x = (double)__ldg(v + i);
-      s1 += x;
-      s2 += x * x;
-    }
-    block_sum2(s1, s2, sRed);
-    if (threadIdx.x == 0) {
-      const double dn = (double)cnt;
-      sStat[0] = (float)(s1 / dn);
-      double var = (s2 - s1 * (s1 / dn)) / (dn - 1.0);
-      if (var < 0.0) var = 0.0;  // rounding can push an exact 0 below 0 (NaN stays NaN)
-      sStat[1] = (float)var;
+__device__ __forceinline__ const float *tree_vals(const TreeLevelArgs &a, int t) {
+  // Level 0 reads the root values straight from P (column t*(gd-1)).
+  return a.level == 0 ? a.P + (int64_t)t * (a.gd - 1) * a.n : a.val_in + (int64_t)t * a.n;
+}
+
+// ------------------------------------------------------------------ plan
+__global__ void __launch_bounds__(1024) k_plan(TreeLevelArgs a) {
+  __shared__ int warp_tot[32];
+  const int G = a.T << a.level;  // nodes of all trees
+  const int per = (G + 1023) / 1024;
+  const int g0 = threadIdx.x * per;
+  int cnt = 0;
+  for (int i = 0; i < per; ++i) {
+    const int g = g0 + i;
+    if (g < G) {
+      const NodeRange r = node_range(a, g);
+      cnt += (int)ceil_div(r.hi - r.lo, kUnit);
     }
   }
-  for (int i = threadIdx.x; i < kWarps * kBins; i += kThreads) (&sHist[0][0])[i] = 0u;
+  // block-wide exclusive scan of cnt
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[w] = x;
   __syncthreads();
-  if (threadIdx.x == 0) node_bounds(sStat[0], __fsqrt_rn(sStat[1]), sD);
+  if (w == 0) {
+    int v = warp_tot[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, v, o);
+      if (lane >= o) v += y;
+    }
+    warp_tot[lane] = v;
+  }
   __syncthreads();
+  int base = x - cnt + (w > 0 ? warp_tot[w - 1] : 0);
+  for (int i = 0; i < per; ++i) {
+    const int g = g0 + i;
+    if (g >= G) break;
+    const NodeRange r = node_range(a, g);
+    const int nu = (int)ceil_div(r.hi - r.lo, kUnit);
+    a.node_ubase[g] = base;
+    for (int c = 0; c < nu; ++c) {
+      a.unit_node[base + c] = g;
+      a.unit_lo[base + c] = (int32_t)(r.lo + (int64_t)c * kUnit);
+    }
+    base += nu;
+  }
+  if (threadIdx.x == 1023) {
+    a.node_ubase[G] = base;
+    *a.n_units = base;
+  }
+}
 
-  // 2. histogram (integer counts: order does not matter)
+// ------------------------------------------------------------------ exact stats
+// Sequential FP32 sum of v[0..n) (or of (v - mu)^2), warp 0 adding from a
+// shared-memory double buffer that warps 1..7 fill.  All of warp 0 computes
+// the same chain; every thread returns it after the final barrier.
+template <bool kSq>
+__device__ float block_chain(const float *__restrict__ v, int64_t n, float mu, float *buf,
+                             float *result) {
+  const int warp = threadIdx.x >> 5;
+  const int64_t chunks = ceil_div(n, kChainChunk);
+  float s = 0.0f;
+  auto load = [&](int64_t c) {
+    float *dst = buf + (c & 1) * kChainChunk;
+    const int64_t base = c * kChainChunk;
+    const int len = (int)min64(kChainChunk, n - base);
+    for (int i = threadIdx.x - 32; i < len; i += kThreads - 32) {
+      float x = __ldg(v + base + i);
+      if (kSq) {
+        const float df = __fsub_rn(x, mu);
+        x = __fmul_rn(df, df);
+      }
+      dst[i] = x;
+    }
+  };
+  if (warp != 0 && chunks > 0) load(0);
+  for (int64_t c = 0; c < chunks; ++c) {
+    __syncthreads();  // buffer c complete; buffer c+1 free
+    if (warp != 0) {
+      if (c + 1 < chunks) load(c + 1);
+    } else {
+      const float *src = buf + (c & 1) * kChainChunk;
+      const int len = (int)min64(kChainChunk, n - c * kChainChunk);
+      const int len4 = len & ~3;
+      const float4 *src4 = reinterpret_cast<const float4 *>(src);
+#pragma unroll 8
+      for (int i = 0; i < len4 / 4; ++i) {
+        const float4 q = src4[i];
+        s = __fadd_rn(s, q.x);
+        s = __fadd_rn(s, q.y);
+        s = __fadd_rn(s, q.z);
+        s = __fadd_rn(s, q.w);
+      }
+      for (int i = len4; i < len; ++i) s = __fadd_rn(s, src[i]);
+    }
+  }
+  if (threadIdx.x == 0) *result = s;
+  __syncthreads();
+  return *result;
+}
+
+__global__ void __launch_bounds__(kThreads) k_stats_exact(TreeLevelArgs a) {
+  __shared__ __align__(16) float buf[2 * kChainChunk];
+  __shared__ float sh[2];
+  const int g = blockIdx.x;
+  const int t = g >> a.level;
+  const NodeRange r = node_range(a, g);
+  const int64_t cnt = r.hi - r.lo;
+  const float *v = tree_vals(a, t) + r.lo;
+  const float sum = block_chain<false>(v, cnt, 0.0f, buf, &sh[0]);     // :137-142
+  const float mu = __fdiv_rn(sum, __int2float_rn((int)cnt));          // :164
+  const float sq = block_chain<true>(v, cnt, mu, buf, &sh[1]);        // :186-192
+  if (threadIdx.x == 0) {
+    const float var = __fdiv_rn(sq, __int2float_rn((int)cnt - 1));    // :201
+    float Dl[kBins];
+    node_bounds(mu, __fsqrt_rn(var), Dl);
+    float *D = a.node_D + (int64_t)g * kBins;
+#pragma unroll
+    for (int j = 0; j < kBins; ++j) D[j] = Dl[j];
+  }
+}
+
+// ------------------------------------------------------------------ fast stats
+__global__ void __launch_bounds__(kThreads) k_stats_partial(TreeLevelArgs a) {
+  __shared__ double sh[2 * kWarps];
+  const int u = blockIdx.x;
+  if (u >= *a.n_units) return;
+  const int g = a.unit_node[u];
+  const int t = g >> a.level;
+  const NodeRange r = node_range(a, g);
+  const int64_t lo = a.unit_lo[u];
+  const int len = (int)min64(kUnit, r.hi - lo);
+  const float *v = tree_vals(a, t) + lo;
+  double s1 = 0.0, s2 = 0.0;
+  for (int i = threadIdx.x; i < len; i += kThreads) {
+    const double x = (double)__ldg(v + i);
+    s1 += x;
+    s2 += x * x;
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s1 += __shfl_down_sync(kFull, s1, o);
+    s2 += __shfl_down_sync(kFull, s2, o);
+  }
+  if (lane == 0) {
+    sh[2 * w] = s1;
+    sh[2 * w + 1] = s2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t1 = 0.0, t2 = 0.0;
+    for (int i = 0; i < kWarps; ++i) {
+      t1 += sh[2 * i];
+      t2 += sh[2 * i + 1];
+    }
+    a.unit_s[2 * u] = t1;
+    a.unit_s[2 * u + 1] = t2;
+  }
+}
+
+__global__ void k_bounds_fast(TreeLevelArgs a) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (a.T << a.level)) return;
+  const NodeRange r = node_range(a, g);
+  double s1 = 0.0, s2 = 0.0;
+  for (int u = a.node_ubase[g]; u < a.node_ubase[g + 1]; ++u) {
+    s1 += a.unit_s[2 * u];
+    s2 += a.unit_s[2 * u + 1];
+  }
+  const double dn = (double)(r.hi - r.lo);
+  double var = (s2 - s1 * (s1 / dn)) / (dn - 1.0);
+  if (var < 0.0) var = 0.0;  // rounding can push a zero variance below 0 (NaN stays NaN)
+  float Dl[kBins];
+  node_bounds((float)(s1 / dn), __fsqrt_rn((float)var), Dl);
+  float *D = a.node_D + (int64_t)g * kBins;
+#pragma unroll
+  for (int j = 0; j < kBins; ++j) D[j] = Dl[j];
+}
+
+// ------------------------------------------------------------------ histogram
+__global__ void __launch_bounds__(kThreads) k_hist(TreeLevelArgs a) {
+  __shared__ unsigned hist[kWarps][kBins];
+  __shared__ float Ds[kBins];
+  const int u = blockIdx.x;
+  if (u >= *a.n_units) return;
+  const int g = a.unit_node[u];
+  const int t = g >> a.level;
+  const NodeRange r = node_range(a, g);
+  const int64_t lo = a.unit_lo[u];
+  const int len = (int)min64(kUnit, r.hi - lo);
+  const float *v = tree_vals(a, t) + lo;
+  if (threadIdx.x < kBins) Ds[threadIdx.x] = a.node_D[(int64_t)g * kBins + threadIdx.x];
+  for (int i = threadIdx.x; i < kWarps * kBins; i += kThreads) (&hist[0][0])[i] = 0u;
+  __syncthreads();
   float D[kBins];
 #pragma unroll
-  for (int j = 0; j < kBins; ++j) D[j] = sD[j];
-  for (int64_t i = threadIdx.x; i < cnt; i += kThreads) atomicAdd(&sHist[warp][bin_of(D, __ldg(v + i))], 1u);
+  for (int j = 0; j < kBins; ++j) D[j] = Ds[j];
+  const int w = threadIdx.x >> 5;
+  for (int i = threadIdx.x; i < len; i += kThreads) atomicAdd(&hist[w][bin_of(D, __ldg(v + i))], 1u);
   __syncthreads();
   if (threadIdx.x < kBins) {
     unsigned tot = 0;
-    for (int w = 0; w < kWarps; ++w) tot += sHist[w][threadIdx.x];
-    sHist[0][threadIdx.x] = tot;
+    for (int k = 0; k < kWarps; ++k) tot += hist[k][threadIdx.x];
+    a.unit_hist[(int64_t)u * kBins + threadIdx.x] = tot;
   }
-  __syncthreads();
+}
 
-  // 3. median
-  if (threadIdx.x == 0) {
-    const float med = node_median(sD, sHist[0], cnt);
-    sStat[0] = med;
-    if (a.medians) a.medians[(int64_t)t * ((1 << (a.gd - 1)) - 1) + (nodes - 1) + node] = med;
+// ------------------------------------------------------------------ median
+__global__ void k_median(TreeLevelArgs a) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (a.T << a.level)) return;
+  const NodeRange r = node_range(a, g);
+  unsigned h[kBins];
+#pragma unroll
+  for (int j = 0; j < kBins; ++j) h[j] = 0u;
+  for (int u = a.node_ubase[g]; u < a.node_ubase[g + 1]; ++u)
+#pragma unroll
+    for (int j = 0; j < kBins; ++j) h[j] += a.unit_hist[(int64_t)u * kBins + j];
+  float D[kBins];
+#pragma unroll
+  for (int j = 0; j < kBins; ++j) D[j] = a.node_D[(int64_t)g * kBins + j];
+  const float med = node_median(D, h, r.hi - r.lo);
+  a.node_med[g] = med;
+  if (a.medians) {
+    const int nodes = 1 << a.level, t = g >> a.level, s = g & (nodes - 1);
+    a.medians[(int64_t)t * ((1 << (a.gd - 1)) - 1) + (nodes - 1) + s] = med;
   }
-  __syncthreads();
-  const float med = sStat[0];
+}
 
-  // 4. stable partition: value <= median goes left (drpt_global.cpp:308)
+// ------------------------------------------------------------------ count
+__global__ void __launch_bounds__(kThreads) k_count(TreeLevelArgs a) {
+  __shared__ int sh[kWarps];
+  const int u = blockIdx.x;
+  if (u >= *a.n_units) return;
+  const int g = a.unit_node[u];
+  const int t = g >> a.level;
+  const NodeRange r = node_range(a, g);
+  const int64_t lo = a.unit_lo[u];
+  const int len = (int)min64(kUnit, r.hi - lo);
+  const float *v = tree_vals(a, t) + lo;
+  const float med = a.node_med[g];
   int c = 0;
-  for (int64_t i = threadIdx.x; i < cnt; i += kThreads) c += (__ldg(v + i) <= med) ? 1 : 0;
-  const int64_t nleft = block_count(c, sCnt);
-
-  const int32_t *oin = a.ord_in ? a.ord_in + (int64_t)t * a.n + lo : nullptr;
-  int32_t *oout = a.ord_out + (int64_t)t * a.n + lo;
-  float *vout = a.val_out ? a.val_out + (int64_t)t * a.n + lo : nullptr;
-  const float *pnext =
-      vout ? a.P + ((int64_t)t * (a.gd - 1) + a.level + 1) * a.n : nullptr;
-  int64_t lbase = 0, rbase = 0;
-  for (int64_t b = 0; b < cnt; b += kThreads) {
-    const int64_t i = b + threadIdx.x;
-    const bool valid = i < cnt;
-    const bool left = valid && __ldg(v + i) <= med;
-    const unsigned bl = __ballot_sync(kFull, left);
-    const unsigned bv = __ballot_sync(kFull, valid);
-    if (lane == 0) sCnt[warp] = __popc(bl) | (__popc(bv) << 16);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int accl = 0, accv = 0;
-      for (int w = 0; w < kWarps; ++w) {
-        sScan[w] = accl | (accv << 16);
-        accl += sCnt[w] & 0xffff;
-        accv += sCnt[w] >> 16;
-      }
-      sScan[kWarps] = accl | (accv << 16);
-    }
-    __syncthreads();
-    const unsigned lt = (1u << lane) - 1u;
-    const int wl = sScan[warp] & 0xffff, wv = sScan[warp] >> 16;
-    const int rl = wl + __popc(bl & lt);                  // left-goers before i in the chunk
-    const int rr = (wv + __popc(bv & lt)) - rl;            // right-goers before i
-    if (valid) {
-      const int64_t pos = left ? lbase + rl : nleft + rbase + rr;
-      const int32_t id = oin ? __ldg(oin + i) : (int32_t)(lo + i);
-      oout[pos] = id;
-      if (vout) vout[pos] = __ldg(pnext + id);
-    }
-    const int tl = sScan[kWarps] & 0xffff, tv = sScan[kWarps] >> 16;
-    lbase += tl;
-    rbase += tv - tl;
-    __syncthreads();
-  }
+  for (int i = threadIdx.x; i < len; i += kThreads) c += (__ldg(v + i) <= med) ? 1 : 0;  // :308
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = c;
+  __syncthreads();
   if (threadIdx.x == 0) {
-    int32_t *oo = a.off_out + (int64_t)t * (2 * nodes + 1);
-    oo[2 * node] = (int32_t)lo;
-    oo[2 * node + 1] = (int32_t)(lo + nleft);
-    if (node == nodes - 1) oo[2 * nodes] = (int32_t)hi;
+    int tot = 0;
+    for (int k = 0; k < kWarps; ++k) tot += sh[k];
+    a.unit_left[u] = tot;
+  }
+}
+
+// ------------------------------------------------------------------ node scan
+__global__ void k_node_scan(TreeLevelArgs a) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (a.T << a.level)) return;
+  const NodeRange r = node_range(a, g);
+  int acc = 0;
+  for (int u = a.node_ubase[g]; u < a.node_ubase[g + 1]; ++u) {
+    const int c = a.unit_left[u];
+    a.unit_lbase[u] = acc;
+    acc += c;
+  }
+  a.node_nleft[g] = acc;
+  const int nodes = 1 << a.level, t = g >> a.level, s = g & (nodes - 1);
+  int32_t *oo = a.off_out + (int64_t)t * (2 * nodes + 1);
+  oo[2 * s] = (int32_t)r.lo;
+  oo[2 * s + 1] = (int32_t)(r.lo + acc);
+  if (s == nodes - 1) oo[2 * nodes] = (int32_t)r.hi;
+}
+
+// ------------------------------------------------------------------ scatter
+__global__ void __launch_bounds__(kThreads) k_scatter(TreeLevelArgs a) {
+  __shared__ int32_t sid[kUnit];
+  __shared__ float sval[kUnit];
+  __shared__ int wsum[kWarps];
+  const int u = blockIdx.x;
+  if (u >= *a.n_units) return;
+  const int g = a.unit_node[u];
+  const int t = g >> a.level;
+  const NodeRange r = node_range(a, g);
+  const int64_t lo = a.unit_lo[u];
+  const int len = (int)min64(kUnit, r.hi - lo);
+  const float *v = tree_vals(a, t) + lo;
+  const float med = a.node_med[g];
+  // each thread owns kPer consecutive positions
+  const int p0 = threadIdx.x * kPer;
+  unsigned mask = 0;
+  int my = 0;
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int p = p0 + j;
+    if (p < len && __ldg(v + p) <= med) {
+      mask |= 1u << j;
+      ++my;
+    }
+  }
+  // exclusive scan of the per-thread left counts
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = my;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  int wbase = 0, ltot = 0;
+  for (int k = 0; k < kWarps; ++k) {
+    if (k < w) wbase += wsum[k];
+    ltot += wsum[k];
+  }
+  int lrank = wbase + x - my;            // left-goers before p0 in the unit
+  int rrank = ltot + (p0 - lrank);       // slot of this thread's first right-goer
+  const int32_t *oin = a.ord_in ? a.ord_in + (int64_t)t * a.n + lo : nullptr;
+  const bool want_val = a.val_out != nullptr;
+  const float *pnext = want_val ? a.P + ((int64_t)t * (a.gd - 1) + a.level + 1) * a.n : nullptr;
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int p = p0 + j;
+    if (p < len) {
+      const int32_t id = oin ? __ldg(oin + p) : (int32_t)(lo + p);
+      const int slot = ((mask >> j) & 1u) ? lrank++ : rrank++;
+      sid[slot] = id;
+      if (want_val) sval[slot] = __ldg(pnext + id);
+    }
+  }
+  __syncthreads();
+  // left-goers -> [node lo + unit lbase, ...), right-goers -> [node lo + nleft + rbase, ...)
+  const int64_t lbase = r.lo + a.unit_lbase[u];
+  const int64_t rbase = r.lo + a.node_nleft[g] + (lo - r.lo - a.unit_lbase[u]);
+  int32_t *oout = a.ord_out + (int64_t)t * a.n;
+  float *vout = want_val ? a.val_out + (int64_t)t * a.n : nullptr;
+  for (int i = threadIdx.x; i < len; i += kThreads) {
+    const int64_t dst = i < ltot ? lbase + i : rbase + (i - ltot);
+    oout[dst] = sid[i];
+    if (want_val) vout[dst] = sval[i];
   }
 }
 
 }  // namespace
 
-drpt_status launch_level(const LevelArgs &a, cudaStream_t s) {
-  const int64_t blocks = (int64_t)a.T << a.level;
-  if (blocks > 0x7fffffff) {
+drpt_status launch_tree_level(const TreeLevelArgs &a, int64_t max_units, cudaStream_t s) {
+  const int64_t G = (int64_t)a.T << a.level;
+  if (G > (1 << 20) || max_units > 0x7fffffff) {
     set_error("too many tree nodes at level %d", a.level);
     return DRPT_ERR_UNSUPPORTED;
   }
-  // Level 0 reads the root values straight from P (stride (gd-1)*n per tree).
-  const int64_t stride = a.level == 0 ? (int64_t)(a.gd - 1) * a.n : a.n;
-  k_level<<<(unsigned)blocks, kThreads, 0, s>>>(a, stride);
+  const unsigned U = (unsigned)max_units, gn = (unsigned)ceil_div(G, 128);
+  k_plan<<<1, 1024, 0, s>>>(a);
+  if (a.exact) {
+    k_stats_exact<<<(unsigned)G, kThreads, 0, s>>>(a);
+  } else {
+    k_stats_partial<<<U, kThreads, 0, s>>>(a);
+    k_bounds_fast<<<gn, 128, 0, s>>>(a);
+  }
+  k_hist<<<U, kThreads, 0, s>>>(a);
+  k_median<<<gn, 128, 0, s>>>(a);
+  k_count<<<U, kThreads, 0, s>>>(a);
+  k_node_scan<<<gn, 128, 0, s>>>(a);
+  k_scatter<<<U, kThreads, 0, s>>>(a);
   DRPT_LAUNCH_CHECK();
   return DRPT_OK;
 }
+
+int64_t tree_level_max_units(int64_t n, int T, int level) {
+  return (int64_t)T * (ceil_div(n, kUnit) + ((int64_t)1 << level));
+}
+
+int tree_level_kernels(int exact) { return exact ? 7 : 8; }
 
 }  // namespace drpt

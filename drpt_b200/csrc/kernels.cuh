@@ -18,23 +18,34 @@ drpt_status launch_project(const void *X, int dtype, int64_t n, int d, const Csc
                            float *P, cudaStream_t s);
 
 // ---- K2-K4: one global-tree level of all trees (k_tree.cu) ---------------
-struct LevelArgs {
+struct TreeLevelArgs {
   const float *P;          // projected columns, (T*(gd-1)) x n
   int64_t n;
   int T, gd, level;
-  const int32_t *ord_in;   // T x n, grouped by node, ascending within a node
-  const float *val_in;     // T x n, the level's value of ord_in[.]
-  const int32_t *off_in;   // T x (2^level + 1)
+  const int32_t *ord_in;   // T x n grouped by node (nullptr at level 0: identity)
+  const float *val_in;     // T x n, the level's value of ord_in[.] (unused at level 0)
+  const int32_t *off_in;   // T x (2^level + 1) (nullptr at level 0: {0, n})
   int32_t *ord_out;        // T x n, grouped by child
-  float *val_out;          // T x n, next level's value (unused at the last level)
+  float *val_out;          // T x n, next level's value (nullptr at the last level)
   int32_t *off_out;        // T x (2^(level+1) + 1)
   float *medians;          // T x (2^(gd-1) - 1) heap order, or nullptr
   int exact;               // sequential FP32 statistics
+  // scratch (G = T * 2^level nodes, U = tree_level_max_units units)
+  int32_t *node_ubase;     // G + 1
+  int32_t *unit_node;      // U
+  int32_t *unit_lo;        // U
+  int32_t *n_units;        // 1
+  float *node_D;           // G x 16
+  double *unit_s;          // 2U
+  unsigned *unit_hist;     // U x 16
+  float *node_med;         // G
+  int32_t *unit_left;      // U
+  int32_t *unit_lbase;     // U
+  int32_t *node_nleft;     // G
 };
-drpt_status launch_level(const LevelArgs &a, cudaStream_t s);
-// val_out[t][i] = P[t*(gd-1)][i], ord_out[t][i] = i, off[t] = {0, n}
-drpt_status launch_tree_init(const float *P, int64_t n, int T, int gd, int32_t *ord,
-                             float *val, int32_t *off, cudaStream_t s);
+drpt_status launch_tree_level(const TreeLevelArgs &a, int64_t max_units, cudaStream_t s);
+int64_t tree_level_max_units(int64_t n, int T, int level);
+int tree_level_kernels(int exact);
 
 // ---- K5: positional local split (k_local.cu) ------------------------------
 struct LocalArgs {
@@ -63,6 +74,7 @@ struct LeafKnnArgs {
   float *cand_dist;            // n x T x k
 };
 drpt_status launch_leaf_knn_exact(const LeafKnnArgs &a, cudaStream_t s);
+int leaf_knn_exact_kernels();
 
 // ---- K7: cross-tree merge (k_merge.cu) -------------------------------------
 drpt_status launch_merge(const int32_t *cand_idx, const float *cand_dist, int64_t n, int T, int k,

@@ -1,0 +1,36 @@
+"""A small, self-contained build for profiling one kernel under ncu.
+
+    python -m drpt_b200.profile_case --n 262144 --dim 128 --trees 4 --mode exact --reps 2
+
+Same data distribution as the benchmark workload (Gaussian clusters,
+centres U[0,200]^d, sigma 12, clipped to [0,255]), fewer points and trees so
+that a capture of one or two launches ends within a minute.
+"""
+from __future__ import annotations
+
+import argparse
+
+import torch
+
+from drpt_b200 import build_graph, synth
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=262_144)
+    ap.add_argument("--dim", type=int, default=128)
+    ap.add_argument("--trees", type=int, default=4)
+    ap.add_argument("--nn", type=int, default=10)
+    ap.add_argument("--mode", default="exact")
+    ap.add_argument("--reps", type=int, default=2)
+    args = ap.parse_args()
+    X = synth.clustered_f32(args.n, args.dim, n_clusters=max(1, args.n // 1000), seed=2)
+    Xd = torch.from_numpy(X).cuda()
+    for _ in range(args.reps):
+        _, _, st = build_graph(Xd, args.trees, args.nn, 12345, mode=args.mode)
+    torch.cuda.synchronize()
+    print({k: round(v, 3) if isinstance(v, float) else v for k, v in st.as_dict().items()})
+
+
+if __name__ == "__main__":
+    main()
