@@ -19,7 +19,7 @@ STATUS_NAMES = {
     6: "DRPT_ERR_CUDA", 7: "DRPT_ERR_TIMEOUT", 8: "DRPT_ERR_UNSUPPORTED",
 }
 DTYPE_F32, DTYPE_U8 = 0, 1
-MODE_EXACT, MODE_FAST = 0, 1
+MODE_EXACT, MODE_FAST, MODE_MIXED = 0, 1, 2
 
 # Every symbol include/drpt_gpu.h declares.
 EXPORTS = [
@@ -46,7 +46,7 @@ class BuildDesc(ctypes.Structure):
         ("density", ctypes.c_double), ("seed", ctypes.c_uint32),
         ("local_seeds", ctypes.POINTER(ctypes.c_uint32)), ("mode", ctypes.c_int32),
         ("data_on_device", ctypes.c_int32), ("out_on_device", ctypes.c_int32),
-        ("stream", ctypes.c_void_p),
+        ("stream", ctypes.c_void_p), ("leaf_size", ctypes.c_int32), ("reserved", ctypes.c_int32),
     ]
 
 

@@ -305,7 +305,7 @@ drpt_status check_common(const drpt_build_desc *d) {
   if (!d) return DRPT_ERR_INVALID_ARG;
   if (d->n < 2 || d->n > INT32_MAX || d->d <= 0 || d->ntrees <= 0 || d->nn <= 0 ||
       (d->dtype != DRPT_DTYPE_F32 && d->dtype != DRPT_DTYPE_U8) || !(d->tree_depth_ratio > 0) ||
-      (d->mode != DRPT_MODE_EXACT && d->mode != DRPT_MODE_FAST)) {
+      (d->mode != DRPT_MODE_EXACT && d->mode != DRPT_MODE_FAST && d->mode != DRPT_MODE_MIXED)) {
     set_error("invalid descriptor (n=%lld d=%d ntrees=%d nn=%d dtype=%d mode=%d)",
               (long long)d->n, d->d, d->ntrees, d->nn, d->dtype, d->mode);
     return DRPT_ERR_INVALID_ARG;
@@ -313,6 +313,131 @@ drpt_status check_common(const drpt_build_desc *d) {
   if (d->nn > kMaxK) {
     set_error("nn = %d larger than %d", d->nn, kMaxK);
     return DRPT_ERR_UNSUPPORTED;
+  }
+  return DRPT_OK;
+}
+
+// Mixed-precision pipeline (DRPT_MODE_MIXED): global trees with fast
+// statistics grown to leaves of about `leaf_size` points, BF16 tensor-core
+// brute force of every global leaf, cross-tree merge of the approximate
+// candidates, exact FP32 re-rank with the FP64 boundary check.
+drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, int32_t *oi,
+                      float *od, drpt_stats *stats, cudaStream_t s) {
+  const int64_t n = desc->n;
+  const int d = desc->d, T = desc->ntrees, nn = desc->nn;
+  if (nn > 16) {
+    set_error("mixed mode supports nn <= 16 (got %d)", nn);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  const int d_pad = (d + 63) / 64 * 64;
+  if (d_pad > 256) {
+    set_error("mixed mode supports d <= 256 (got %d)", d);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  const int leaf_size = desc->leaf_size > 0 ? desc->leaf_size : 512;
+  // leaves = 2^(gd-1) >= n / leaf_size
+  int gd = 1;
+  while (gd < 30 && ((int64_t)1 << (gd - 1)) * leaf_size < n) ++gd;
+  if (gd > std::log2((double)n)) {
+    set_error("mixed mode: global depth %d outside [1, log2(%lld)]", gd, (long long)n);
+    return DRPT_ERR_DEPTH_OUT_OF_RANGE;
+  }
+  const int nleaf = 1 << (gd - 1);
+  const int kp = nn <= 10 ? 16 : 32;
+  const int K2 = 2 * nn;
+  const int L = gd * T;
+  const float density = (float)(desc->density == 0 ? 1.0 / std::sqrt((double)d) : desc->density);
+  cudaEvent_t *ev = c->ev;
+  const int launches0 = c->launches;
+  DRPT_CUDA(cudaEventRecord(ev[1], s));
+
+  std::vector<float> B((size_t)d * L);
+  host_projection_matrix(desc->seed, d, L, density, B.data());
+  std::vector<int32_t> cols;
+  for (int t = 0; t < T; ++t)
+    for (int l = 0; l + 1 < gd; ++l) cols.push_back(t * gd + l);
+  float *P = nullptr;
+  DRPT_TRY(ws_get(c, "P", std::max<size_t>(cols.size(), 1) * n, &P));
+  if (!cols.empty()) DRPT_TRY(project_cols(c, X, desc->dtype, n, d, B.data(), L, cols, P, s));
+  int32_t *order, *goff;
+  DRPT_TRY(global_trees(c, P, n, T, gd, 0, nullptr, &order, &goff, s));
+  DRPT_CUDA(cudaEventRecord(ev[2], s));
+
+  MixedTreeArgs a{};
+  a.X = X;
+  a.dtype = desc->dtype;
+  a.n = n;
+  a.d = d;
+  a.d_pad = d_pad;
+  a.nleaf = nleaf;
+  a.T = T;
+  a.kp = kp;
+  DRPT_TRY(ws_get(c, "mx_xb", (size_t)n * d_pad, &a.Xb));
+  DRPT_TRY(ws_get(c, "mx_nrm", (size_t)n, &a.nrm));
+  const size_t tiles = (size_t)ceil_div(n, 128) + nleaf;
+  DRPT_TRY(ws_get(c, "mx_tile_leaf", tiles, &a.tile_leaf));
+  DRPT_TRY(ws_get(c, "mx_tile_r0", tiles, &a.tile_r0));
+  DRPT_TRY(ws_get(c, "mx_n_tiles", 1, &a.n_tiles));
+  DRPT_TRY(ws_get(c, "mx_err", 1, &a.err));
+  DRPT_TRY(ws_get(c, "cand_idx", (size_t)n * T * kp, &a.cand_idx));
+  DRPT_TRY(ws_get(c, "cand_dist", (size_t)n * T * kp, &a.cand_dist));
+  DRPT_CUDA(cudaMemsetAsync(a.err, 0, sizeof(int), s));
+  DRPT_CUDA(cudaEventRecord(ev[3], s));
+  for (int t = 0; t < T; ++t) {
+    a.tree = t;
+    a.order = order + (size_t)t * n;
+    a.goff = goff + (size_t)t * (nleaf + 1);
+    DRPT_TRY(launch_leaf_center(a, s));
+    DRPT_TRY(launch_leaf_mma(a, s));
+    c->launches += 3;
+  }
+  DRPT_CUDA(cudaEventRecord(ev[4], s));
+  int32_t *midx;
+  float *mdist;
+  DRPT_TRY(ws_get(c, "mx_merged_idx", (size_t)n * K2, &midx));
+  DRPT_TRY(ws_get(c, "mx_merged_dist", (size_t)n * K2, &mdist));
+  DRPT_TRY(launch_merge(a.cand_idx, a.cand_dist, n, T, kp, K2, midx, mdist, s));
+  // Re-rank in the leaf order of the last tree: a point's candidates are
+  // mostly its leaf-mates there, so their rows stay in L2.
+  DRPT_TRY(launch_rerank(X, desc->dtype, d, order + (size_t)(T - 1) * n, n, midx, K2, nn, oi, od,
+                         s));
+  c->launches += 2;
+  DRPT_CUDA(cudaEventRecord(ev[5], s));
+  int err = 0;
+  DRPT_CUDA(cudaMemcpyAsync(&err, a.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DRPT_CUDA(cudaStreamSynchronize(s));
+  if (err) {
+    set_error("a bounded wait in the tensor-core leaf kernel gave up");
+    return DRPT_ERR_TIMEOUT;
+  }
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->tree_depth = gd;
+    stats->global_depth = gd;
+    stats->local_depth = 0;
+    stats->n_global_leaves = nleaf;
+    stats->n_final_leaves = nleaf;
+    // leaf sizes for the work figure
+    std::vector<int32_t> h((size_t)T * (nleaf + 1));
+    DRPT_CUDA(cudaMemcpy(h.data(), goff, h.size() * 4, cudaMemcpyDeviceToHost));
+    int64_t sq = 0, mn = INT64_MAX;
+    int mx = 0;
+    for (int t = 0; t < T; ++t)
+      for (int j = 0; j < nleaf; ++j) {
+        const int64_t m = h[(size_t)t * (nleaf + 1) + j + 1] - h[(size_t)t * (nleaf + 1) + j];
+        sq += m * m;
+        if (m > 0) mn = std::min(mn, m);
+        mx = std::max<int>(mx, (int)m);
+      }
+    stats->sum_leaf_sq = sq;
+    stats->min_global_leaf = mn;
+    stats->max_final_leaf = mx;
+    stats->kernels_launched = c->launches - launches0;
+    stats->ms_project = elapsed(ev[0], ev[1]);  // input copy, if any
+    stats->ms_global = elapsed(ev[1], ev[2]);
+    stats->ms_local = elapsed(ev[2], ev[3]);
+    stats->ms_leaf_knn = elapsed(ev[3], ev[4]);
+    stats->ms_merge = elapsed(ev[4], ev[5]);
   }
   return DRPT_OK;
 }
@@ -395,6 +520,27 @@ drpt_status drpt_build_graph(drpt_ctx *c, const drpt_build_desc *desc, const voi
     X = xd;
   }
 
+  if (desc->mode == DRPT_MODE_MIXED) {
+    int32_t *oi = out_idx;
+    float *od = out_dist;
+    if (!desc->out_on_device) {
+      DRPT_TRY(ws_get(c, "out_idx", (size_t)n * nn, &oi));
+      DRPT_TRY(ws_get(c, "out_dist", (size_t)n * nn, &od));
+    } else if (!od) {
+      DRPT_TRY(ws_get(c, "out_dist", (size_t)n * nn, &od));
+    }
+    DRPT_TRY(run_mixed(c, desc, X, oi, od, stats, s));
+    if (!desc->out_on_device) {
+      DRPT_CUDA(cudaMemcpyAsync(out_idx, oi, (size_t)n * nn * 4, cudaMemcpyDeviceToHost, s));
+      if (out_dist)
+        DRPT_CUDA(cudaMemcpyAsync(out_dist, od, (size_t)n * nn * 4, cudaMemcpyDeviceToHost, s));
+    }
+    DRPT_CUDA(cudaEventRecord(ev[6], s));
+    DRPT_CUDA(cudaEventSynchronize(ev[6]));
+    if (stats) stats->ms_total = elapsed(ev[0], ev[6]);
+    return DRPT_OK;
+  }
+
   // K1: projection on the columns the global trees split on.
   std::vector<float> B((size_t)d * L);
   host_projection_matrix(desc->seed, d, L, density, B.data());
@@ -445,7 +591,7 @@ drpt_status drpt_build_graph(drpt_ctx *c, const drpt_build_desc *desc, const voi
   } else if (!od) {
     DRPT_TRY(ws_get(c, "out_dist", (size_t)n * nn, &od));
   }
-  DRPT_TRY(launch_merge(cidx, cdist, n, T, nn, oi, od, s));
+  DRPT_TRY(launch_merge(cidx, cdist, n, T, nn, nn, oi, od, s));
   c->launches += 1;
   DRPT_CUDA(cudaEventRecord(ev[5], s));
   if (!desc->out_on_device) {
@@ -534,7 +680,7 @@ drpt_status drpt_merge_candidates(drpt_ctx *c, const int32_t *cand_idx, const fl
   if (!c || !cand_idx || !cand_dist || !out_idx || !out_dist || n <= 0 || T <= 0)
     return DRPT_ERR_INVALID_ARG;
   DRPT_CUDA(cudaSetDevice(c->device));
-  return launch_merge(cand_idx, cand_dist, n, T, k, out_idx, out_dist, (cudaStream_t)stream);
+  return launch_merge(cand_idx, cand_dist, n, T, k, k, out_idx, out_dist, (cudaStream_t)stream);
 }
 
 }  // extern "C"

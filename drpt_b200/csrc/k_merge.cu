@@ -8,7 +8,7 @@
 // always meets its twin at the same sort position.
 //
 // One warp per point: lane j holds slot j of the running list (k <= 32) or
-// slots j and j+32 (k <= 64).  Candidates are streamed tree by tree; a
+// slots j and j+32 (k <= 64); each tree contributes a list of `lk` entries.  Candidates are streamed tree by tree; a
 // candidate enters when it beats the current k-th entry and is not already
 // present, and the lanes shift to make room.
 #include "kernels.cuh"
@@ -25,7 +25,7 @@ __device__ __forceinline__ bool before(float da, int32_t ia, float db, int32_t i
 template <int S>  // slots per lane
 __global__ void __launch_bounds__(kThreads) k_merge(const int32_t *__restrict__ ci,
                                                     const float *__restrict__ cd, int64_t n, int T,
-                                                    int k, int32_t *__restrict__ oi,
+                                                    int lk, int k, int32_t *__restrict__ oi,
                                                     float *__restrict__ od) {
   const int lane = threadIdx.x & 31;
   const int64_t p = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
@@ -42,17 +42,17 @@ __global__ void __launch_bounds__(kThreads) k_merge(const int32_t *__restrict__ 
   // Tree by tree: each list is sorted, so once an entry fails to beat the
   // current k-th, the rest of that list cannot enter either.
   for (int t = 0; t < T; ++t) {
-    const int32_t *pi = ci + (p * T + t) * k;
-    const float *pd = cd + (p * T + t) * k;
+    const int32_t *pi = ci + (p * T + t) * lk;
+    const float *pd = cd + (p * T + t) * lk;
     float ld[S];
     int32_t li[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
       const int e = s * 32 + lane;
-      ld[s] = e < k ? __ldg(pd + e) : inf;
-      li[s] = e < k ? __ldg(pi + e) : -1;
+      ld[s] = e < lk ? __ldg(pd + e) : inf;
+      li[s] = e < lk ? __ldg(pi + e) : -1;
     }
-    for (int j = 0; j < k; ++j) {
+    for (int j = 0; j < lk; ++j) {
       float cdv = inf;
       int32_t civ = -1;
 #pragma unroll
@@ -124,18 +124,18 @@ __global__ void __launch_bounds__(kThreads) k_merge(const int32_t *__restrict__ 
 
 }  // namespace
 
-drpt_status launch_merge(const int32_t *cand_idx, const float *cand_dist, int64_t n, int T, int k,
-                         int32_t *out_idx, float *out_dist, cudaStream_t s) {
-  if (k <= 0 || k > kMaxK) {
+drpt_status launch_merge(const int32_t *cand_idx, const float *cand_dist, int64_t n, int T, int lk,
+                         int k, int32_t *out_idx, float *out_dist, cudaStream_t s) {
+  if (k <= 0 || k > kMaxK || lk <= 0 || lk > kMaxK) {
     set_error("merge: k = %d outside [1, %d]", k, kMaxK);
     return DRPT_ERR_UNSUPPORTED;
   }
   if (n <= 0) return DRPT_OK;
   const unsigned grid = (unsigned)ceil_div(n * 32, kThreads);
-  if (k <= 32)
-    k_merge<1><<<grid, kThreads, 0, s>>>(cand_idx, cand_dist, n, T, k, out_idx, out_dist);
+  if (k <= 32 && lk <= 32)
+    k_merge<1><<<grid, kThreads, 0, s>>>(cand_idx, cand_dist, n, T, lk, k, out_idx, out_dist);
   else
-    k_merge<2><<<grid, kThreads, 0, s>>>(cand_idx, cand_dist, n, T, k, out_idx, out_dist);
+    k_merge<2><<<grid, kThreads, 0, s>>>(cand_idx, cand_dist, n, T, lk, k, out_idx, out_dist);
   DRPT_LAUNCH_CHECK();
   return DRPT_OK;
 }

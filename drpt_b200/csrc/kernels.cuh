@@ -1,6 +1,8 @@
 // Launch wrappers of the device kernels (one .cu file each).
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 
 namespace drpt {
@@ -77,7 +79,31 @@ drpt_status launch_leaf_knn_exact(const LeafKnnArgs &a, cudaStream_t s);
 int leaf_knn_exact_kernels();
 
 // ---- K7: cross-tree merge (k_merge.cu) -------------------------------------
-drpt_status launch_merge(const int32_t *cand_idx, const float *cand_dist, int64_t n, int T, int k,
-                         int32_t *out_idx, float *out_dist, cudaStream_t s);
+// T sorted lists of `lk` entries per point (n x T x lk) -> the k best distinct.
+drpt_status launch_merge(const int32_t *cand_idx, const float *cand_dist, int64_t n, int T, int lk,
+                         int k, int32_t *out_idx, float *out_dist, cudaStream_t s);
+
+// ---- K8-K11: mixed-precision leaf brute force (k_mixed.cu) ---------------------
+struct MixedTreeArgs {
+  const void *X;
+  int dtype;
+  int64_t n;
+  int d, d_pad;
+  const int32_t *order;      // this tree's global-leaf order (n)
+  const int32_t *goff;       // this tree's leaf starts (nleaf + 1)
+  int nleaf;
+  int T, tree, kp;           // trees, this tree, candidates kept per tree
+  __nv_bfloat16 *Xb;         // n x d_pad, centred rows in leaf order
+  float *nrm;                // n, squared norms of the BF16 rows
+  int32_t *tile_leaf, *tile_r0, *n_tiles;  // n / 128 + nleaf
+  int32_t *cand_idx;         // n x T x kp
+  float *cand_dist;          // n x T x kp (approximate squared distances)
+  int *err;                  // set when a bounded wait gave up
+};
+drpt_status launch_leaf_center(const MixedTreeArgs &a, cudaStream_t s);
+drpt_status launch_leaf_mma(const MixedTreeArgs &a, cudaStream_t s);
+drpt_status launch_rerank(const void *X, int dtype, int d, const int32_t *visit, int64_t n,
+                          const int32_t *cand, int K2, int k, int32_t *out_idx, float *out_dist,
+                          cudaStream_t s);
 
 }  // namespace drpt

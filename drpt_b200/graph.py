@@ -60,7 +60,7 @@ def global_depth(n: int, tree_depth_ratio: float = 0.6, tree_depth: int = 0) -> 
 def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
                 tree_depth_ratio: float = 0.6, local_tree_offset: int = 2, tree_depth: int = 0,
                 density: float = 0.0, local_seeds=None, device: int = 0, stream=None,
-                out=None):
+                out=None, leaf_size: int = 0):
     """k-NN graph of `data` (n x d, uint8 or float32; a NumPy array in host
     memory or a CUDA tensor).  Returns (idx, dist, stats): idx int32 and dist
     float32 of shape (n, nn), each point's nn nearest distinct neighbours other
@@ -83,7 +83,8 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
     if local_seeds is not None:
         seeds_arr = (ctypes.c_uint32 * ntrees)(*[int(s) & 0xFFFFFFFF for s in local_seeds])
         desc.local_seeds = seeds_arr
-    desc.mode = {"exact": _lib.MODE_EXACT, "fast": _lib.MODE_FAST}[mode]
+    desc.mode = {"exact": _lib.MODE_EXACT, "fast": _lib.MODE_FAST, "mixed": _lib.MODE_MIXED}[mode]
+    desc.leaf_size = leaf_size
     desc.data_on_device = 1 if on_dev else 0
     desc.out_on_device = desc.data_on_device
     if on_dev:

@@ -23,11 +23,12 @@ def main() -> None:
     ap.add_argument("--nn", type=int, default=10)
     ap.add_argument("--mode", default="exact")
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--leaf", type=int, default=0, help="mixed mode: target leaf size")
     args = ap.parse_args()
     X = synth.clustered_f32(args.n, args.dim, n_clusters=max(1, args.n // 1000), seed=2)
     Xd = torch.from_numpy(X).cuda()
     for _ in range(args.reps):
-        _, _, st = build_graph(Xd, args.trees, args.nn, 12345, mode=args.mode)
+        _, _, st = build_graph(Xd, args.trees, args.nn, 12345, mode=args.mode, leaf_size=args.leaf)
     torch.cuda.synchronize()
     print({k: round(v, 3) if isinstance(v, float) else v for k, v in st.as_dict().items()})
 

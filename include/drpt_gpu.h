@@ -60,7 +60,14 @@ typedef enum {
   DRPT_MODE_EXACT = 0,
   /* Plain form with parallel (deterministic, FP64) node statistics; same
    * algorithm otherwise.  Not bit-exact in tree assignment. */
-  DRPT_MODE_FAST = 1
+  DRPT_MODE_FAST = 1,
+  /* Mixed-precision form: the same global trees (fast statistics), grown to
+   * leaves of about `leaf_size` points; every global leaf is brute-forced
+   * with BF16 tensor-core Gram tiles (FP32 accumulation) keeping 16 (nn <= 10)
+   * or 32 candidates per tree and point; the merged 2*nn best are re-ranked
+   * with exact FP32 distances and the k-th boundary is checked in FP64.  No
+   * positional local split.  nn <= 16, d <= 256. */
+  DRPT_MODE_MIXED = 2
 } drpt_mode;
 
 typedef struct drpt_ctx drpt_ctx;
@@ -82,6 +89,8 @@ typedef struct {
   int32_t data_on_device;     /* 1: `data` is device memory; 0: host memory */
   int32_t out_on_device;      /* 1: outputs are device memory; 0: host */
   void *stream;               /* cudaStream_t to run on; NULL = legacy default */
+  int32_t leaf_size;          /* mixed mode: target global leaf size (0 = 512) */
+  int32_t reserved;
 } drpt_build_desc;
 
 typedef struct {
