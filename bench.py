@@ -1,14 +1,20 @@
 """Benchmark of the k-NN-graph path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--mode exact|fast] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--mode mixed|exact|fast]
+                    [--impl ours|reference]
 
-Workload (one step = one complete graph build): 1,000,000 x 128 float32
-points, a mixture of 1,000 Gaussian clusters (centres U[0,200]^128, sigma 12,
-clipped to [0,255]), ntrees = 16, nn = 10 -- synthetic data of the shape of
-the fbin workload.  `value` is points/s with the input resident in HBM
-(512 MB, larger than L2, so no flush is needed between steps); `e2e` is the
-same build through the public host-pointer call with the input copied from
-pinned host memory and the neighbour lists copied back, every step.
+Workload (one step = one complete graph build of 1,000,000 x 128 float32
+points, a mixture of 1,000 Gaussian clusters with centres U[0,200]^128,
+sigma 12, clipped to [0,255]; nn = 10; synthetic data of the shape of the
+fbin workload).  The headline form is the mixed-precision one (6 trees,
+global leaves of about 1,024 points, BF16 tensor-core leaf tiles, exact FP32
+re-rank), which reaches recall@10 >= 0.90; beside it, at one GPU, the plain
+FP32 form with the reference's parameters (16 trees, reference-exact) and the
+plain form with enough trees to approach the same recall are timed once.
+`value` is points/s with the input resident in HBM (512 MB, larger than L2,
+so no flush is needed between steps); `e2e` is the same build through the
+public host-pointer call with the input copied from pinned host memory and
+the neighbour lists copied back, every step.
 
 Under torchrun (N > 1) every rank builds an independent graph of its own
 1M-point dataset (the path has no inter-GPU exchange: replicas, weak
@@ -40,12 +46,14 @@ sys.path.insert(0, ROOT)
 
 METRIC = "kNN-graph points/s at recall@10≥0.90, mixed/learned vs plain FP32, 1 B200"
 N_POINTS, DIM, NTREES, NN, N_CLUSTERS = 1_000_000, 128, 16, 10, 1000
+MIXED_TREES, MIXED_LEAF = 6, 1024   # mixed form: trees and target global-leaf size
+PLAIN_MATCH_TREES = 384             # plain form grown towards the mixed form's recall
 SEED_PROJ = 12345
 CPU_SAMPLE = 32_768  # bounded sample for the CPU baseline (about 10-30 s of CPU work)
 REF_STEP_SAMPLE = 16_384  # per timed step of --impl reference
 REF_WARMUP_SAMPLE = 4_096  # per untimed warm-up step of --impl reference
 WORKLOAD = ("1,000,000 x 128 float32 (fbin-shaped), 1000 Gaussian clusters, centres U[0,200]^128, "
-            "sigma 12, clipped to [0,255]; ntrees=16, nn=10")
+            "sigma 12, clipped to [0,255]; nn=10; plain form ntrees=16 (reference parameters)")
 
 
 def _env_int(name, default):
@@ -220,10 +228,11 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--mode", default="exact", choices=["exact", "fast"])
+    ap.add_argument("--mode", default="mixed", choices=["mixed", "exact", "fast"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain-compare", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
@@ -250,9 +259,12 @@ def main():
     Xd = torch.from_numpy(X).to(dev)
     idx = torch.empty((N_POINTS, NN), dtype=torch.int32, device=dev)
     dst = torch.empty((N_POINTS, NN), dtype=torch.float32, device=dev)
+    trees = MIXED_TREES if args.mode == "mixed" else NTREES
+    leaf = MIXED_LEAF if args.mode == "mixed" else 0
 
-    def step():
-        return build_graph(Xd, NTREES, NN, SEED_PROJ + rank, mode=args.mode, out=(idx, dst))[2]
+    def step(mode=args.mode, ntrees=trees, leaf_size=leaf, data=Xd, out=(idx, dst)):
+        return build_graph(data, ntrees, NN, SEED_PROJ + rank, mode=mode, leaf_size=leaf_size,
+                           out=out)[2]
 
     def barrier():
         if world > 1:
@@ -263,7 +275,8 @@ def main():
     torch.cuda.synchronize()
 
     # device-resident timing
-    per_kernel = {"leaf_knn": [], "global": [], "project": [], "merge": [], "local": []}
+    phases = {k: [] for k in ("project", "global", "local", "leaf_knn", "merge", "leaf_mma",
+                              "leaf_stage")}
     launches = 0
     with ClockSampler(local_rank) as clocks:
         barrier()
@@ -272,11 +285,8 @@ def main():
         e0.record(stream)
         for _ in range(args.steps):
             st = step()
-            per_kernel["leaf_knn"].append(st.ms_leaf_knn)
-            per_kernel["global"].append(st.ms_global)
-            per_kernel["project"].append(st.ms_project)
-            per_kernel["merge"].append(st.ms_merge)
-            per_kernel["local"].append(st.ms_local)
+            for k in phases:
+                phases[k].append(getattr(st, "ms_" + k))
             launches += st.kernels_launched
         e1.record(stream)
         torch.cuda.synchronize()
@@ -288,6 +298,11 @@ def main():
         ms = float(t.item())
     clk = clocks.summary()
 
+    # recall@10 on a seeded sample against FP64 exact neighbours
+    q = recall.sample_queries(N_POINTS, 1000, seed=7)
+    true_i, _ = recall.exact_knn_fp64(Xd, q, NN, device=local_rank)
+    rec = recall.recall_at_k(idx.cpu().numpy()[q], true_i)
+
     # end to end through the host-pointer call, pinned buffers
     e2e = None
     if not args.no_e2e:
@@ -295,14 +310,17 @@ def main():
         oi = torch.empty((N_POINTS, NN), dtype=torch.int32).pin_memory()
         od = torch.empty((N_POINTS, NN), dtype=torch.float32).pin_memory()
         xnp, inp, dnp = Xh.numpy(), oi.numpy(), od.numpy()
-        build_graph(xnp, NTREES, NN, SEED_PROJ + rank, mode=args.mode, out=(inp, dnp),
-                    stream=stream.cuda_stream)
+
+        def host_step():
+            build_graph(xnp, trees, NN, SEED_PROJ + rank, mode=args.mode, leaf_size=leaf,
+                        out=(inp, dnp), stream=stream.cuda_stream)
+
+        host_step()
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            build_graph(xnp, NTREES, NN, SEED_PROJ + rank, mode=args.mode, out=(inp, dnp),
-                        stream=stream.cuda_stream)
+            host_step()
         torch.cuda.synchronize()
         e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
         if world > 1:
@@ -313,38 +331,69 @@ def main():
                "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(X.nbytes),
                "d2h_bytes_per_step": int(oi.numel() * 4 + od.numel() * 4)}
 
-    # recall@10 on a seeded sample against FP64 exact neighbours
-    q = recall.sample_queries(N_POINTS, 1000, seed=7)
-    true_i, _ = recall.exact_knn_fp64(Xd, q, NN, device=local_rank)
-    rec = recall.recall_at_k(idx.cpu().numpy()[q], true_i)
+    # the plain FP32 form beside it (one GPU only): reference parameters, and
+    # grown towards the mixed form's recall
+    plain = None
+    if not args.no_plain_compare and world == 1 and args.mode == "mixed":
+        plain = {}
+        for name, mode, ntrees in (("exact_16_trees", "exact", NTREES),
+                                   ("fast_16_trees", "fast", NTREES),
+                                   (f"fast_{PLAIN_MATCH_TREES}_trees", "fast", PLAIN_MATCH_TREES)):
+            pi = torch.empty((N_POINTS, NN), dtype=torch.int32, device=dev)
+            pd = torch.empty((N_POINTS, NN), dtype=torch.float32, device=dev)
+            step(mode, ntrees, 0, Xd, (pi, pd))
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step(mode, ntrees, 0, Xd, (pi, pd))
+            b.record(stream)
+            torch.cuda.synchronize()
+            pms = a.elapsed_time(b)
+            plain[name] = {"points_per_s": N_POINTS / (pms / 1e3), "ms": pms, "ntrees": ntrees,
+                           "recall@10": recall.recall_at_k(pi.cpu().numpy()[q], true_i)}
+            del pi, pd
+        best_plain = max(v["points_per_s"] for v in plain.values() if v["recall@10"] >= rec - 0.02) \
+            if any(v["recall@10"] >= rec - 0.02 for v in plain.values()) else None
+        plain["mixed_over_plain_at_equal_recall"] = (world * N_POINTS / (ms / 1e3)) / best_plain \
+            if best_plain else None
 
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
         return
 
-    # roofline of the dominant kernel (leaf brute force), exact FP32 SIMT:
-    # 3 FP32 operations (subtract, multiply, add) per pair and dimension
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except (OSError, ValueError):
         pass
-    leaf_ms = statistics.median(per_kernel["leaf_knn"])
-    flops = 3.0 * st.sum_leaf_sq * DIM
-    achieved = flops / (leaf_ms * 1e-3) / 1e12
-    sm_mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
-    fp32_peak = 148 * 128 * sm_mhz * 1e6 / 1e12  # one FP32 op per lane per clock (no FMA pairing)
-    traffic = _traffic_per_launch("k_leaf_knn")
-    roofline = {"kernel": "k_leaf_knn (exact FP32 leaf brute force)", "bound": "fp32",
-                "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                "frac": achieved / fp32_peak, "traffic": traffic,
-                "peak_source": "nominal FP32 issue rate (148 SMs x 128 lanes x median SM clock); "
-                               "MEASURED_PEAKS.json holds no FP32 figure",
-                "algorithmic_flops_per_launch": flops,
-                "hbm_bytes_alg_per_launch": float(N_POINTS * NTREES * DIM * 4),
-                "hbm_frac_of_measured": (N_POINTS * NTREES * DIM * 4 / (leaf_ms * 1e-3) / 1e9) /
-                                        peaks.get("hbm_gbs", 6651.7)}
+    if args.mode == "mixed":
+        # dominant kernel: the tensor-core leaf kernel (one launch per tree);
+        # algorithmic work = 2*d multiply-adds per leaf pair
+        mma_ms = statistics.median(phases["leaf_mma"]) / trees
+        flops = 2.0 * DIM * st.sum_leaf_sq / trees
+        achieved = flops / (mma_ms * 1e-3) / 1e12
+        peak = peaks.get("bf16_tflops_sustained", 1414.3)
+        roofline = {"kernel": "k_leaf_mma (BF16 tcgen05 Gram tiles + top-k epilogue), per launch",
+                    "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": _traffic_per_launch("k_leaf_mma"),
+                    "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)",
+                    "algorithmic_flops_per_launch": flops, "ms_per_launch": mma_ms,
+                    "padded_tile_flops_per_launch": 2.0 * 128 * st.mma_pairs_padded / trees,
+                    "note": "the epilogue (threshold filter + bitonic top-k in registers) bounds "
+                            "this kernel, not the tensor pipe"}
+    else:
+        leaf_ms = statistics.median(phases["leaf_knn"])
+        flops = 3.0 * st.sum_leaf_sq * DIM
+        achieved = flops / (leaf_ms * 1e-3) / 1e12
+        sm_mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+        fp32_peak = 148 * 128 * sm_mhz * 1e6 / 1e12
+        roofline = {"kernel": "k_leaf_knn (exact FP32 leaf brute force)", "bound": "fp32",
+                    "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                    "frac": achieved / fp32_peak, "traffic": _traffic_per_launch("k_leaf_knn"),
+                    "peak_source": "nominal FP32 issue rate (148 SMs x 128 lanes x median SM "
+                                   "clock); MEASURED_PEAKS.json holds no FP32 figure",
+                    "algorithmic_flops_per_launch": flops}
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         try:
@@ -356,10 +405,12 @@ def main():
         "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "mode": args.mode, "recall@10": rec,
-                   "recall_sample": 1000, "global_depth": st.global_depth,
-                   "local_depth": st.local_depth, "mean_leaf": st.sum_leaf_sq / (NTREES * N_POINTS),
-                   "phase_ms": {k: statistics.median(v) for k, v in per_kernel.items()},
+        "config": {"workload": WORKLOAD, "mode": args.mode, "ntrees": trees,
+                   "leaf_size": leaf or None, "recall@10": rec, "recall_sample": 1000,
+                   "global_depth": st.global_depth, "local_depth": st.local_depth,
+                   "mean_leaf": st.sum_leaf_sq / (trees * N_POINTS),
+                   "phase_ms": {k: statistics.median(v) for k, v in phases.items()},
+                   "plain_form": plain,
                    "l2": "input 512 MB > 126 MB L2; no flush between steps",
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
         "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e,

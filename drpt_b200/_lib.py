@@ -59,6 +59,8 @@ class Stats(ctypes.Structure):
         ("kernels_launched", ctypes.c_int32), ("reserved", ctypes.c_int32),
         ("ms_project", ctypes.c_float), ("ms_global", ctypes.c_float), ("ms_local", ctypes.c_float),
         ("ms_leaf_knn", ctypes.c_float), ("ms_merge", ctypes.c_float), ("ms_total", ctypes.c_float),
+        ("ms_leaf_mma", ctypes.c_float), ("ms_leaf_stage", ctypes.c_float),
+        ("mma_pairs_padded", ctypes.c_int64),
     ]
 
     def as_dict(self) -> dict:

@@ -33,6 +33,7 @@ struct drpt_ctx {
   std::map<std::string, Buf> bufs;
   std::map<std::pair<int64_t, int>, std::pair<std::vector<int32_t>, std::vector<int32_t>>> perms;
   cudaEvent_t ev[8] = {};
+  std::vector<cudaEvent_t> tev;  // per-tree event pairs (mixed mode)
   int launches = 0;
 };
 
@@ -343,8 +344,7 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
     return DRPT_ERR_DEPTH_OUT_OF_RANGE;
   }
   const int nleaf = 1 << (gd - 1);
-  const int kp = nn <= 10 ? 16 : 32;
-  const int K2 = 2 * nn;
+  const int kp = nn <= 10 ? 16 : 32;  // running candidates per point, re-ranked at the end
   const int L = gd * T;
   const float density = (float)(desc->density == 0 ? 1.0 / std::sqrt((double)d) : desc->density);
   cudaEvent_t *ev = c->ev;
@@ -379,29 +379,32 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
   DRPT_TRY(ws_get(c, "mx_tile_r0", tiles, &a.tile_r0));
   DRPT_TRY(ws_get(c, "mx_n_tiles", 1, &a.n_tiles));
   DRPT_TRY(ws_get(c, "mx_err", 1, &a.err));
-  DRPT_TRY(ws_get(c, "cand_idx", (size_t)n * T * kp, &a.cand_idx));
-  DRPT_TRY(ws_get(c, "cand_dist", (size_t)n * T * kp, &a.cand_dist));
+  DRPT_TRY(ws_get(c, "mx_run_idx", (size_t)n * kp, &a.cand_idx));
+  DRPT_TRY(ws_get(c, "mx_run_dist", (size_t)n * kp, &a.cand_dist));
   DRPT_CUDA(cudaMemsetAsync(a.err, 0, sizeof(int), s));
   DRPT_CUDA(cudaEventRecord(ev[3], s));
+  while ((int)c->tev.size() < 3 * T) {
+    cudaEvent_t e;
+    DRPT_CUDA(cudaEventCreate(&e));
+    c->tev.push_back(e);
+  }
   for (int t = 0; t < T; ++t) {
     a.tree = t;
     a.order = order + (size_t)t * n;
     a.goff = goff + (size_t)t * (nleaf + 1);
+    DRPT_CUDA(cudaEventRecord(c->tev[3 * t], s));
     DRPT_TRY(launch_leaf_center(a, s));
+    DRPT_CUDA(cudaEventRecord(c->tev[3 * t + 1], s));
     DRPT_TRY(launch_leaf_mma(a, s));
+    DRPT_CUDA(cudaEventRecord(c->tev[3 * t + 2], s));
     c->launches += 3;
   }
   DRPT_CUDA(cudaEventRecord(ev[4], s));
-  int32_t *midx;
-  float *mdist;
-  DRPT_TRY(ws_get(c, "mx_merged_idx", (size_t)n * K2, &midx));
-  DRPT_TRY(ws_get(c, "mx_merged_dist", (size_t)n * K2, &mdist));
-  DRPT_TRY(launch_merge(a.cand_idx, a.cand_dist, n, T, kp, K2, midx, mdist, s));
   // Re-rank in the leaf order of the last tree: a point's candidates are
   // mostly its leaf-mates there, so their rows stay in L2.
-  DRPT_TRY(launch_rerank(X, desc->dtype, d, order + (size_t)(T - 1) * n, n, midx, K2, nn, oi, od,
-                         s));
-  c->launches += 2;
+  DRPT_TRY(launch_rerank(X, desc->dtype, d, order + (size_t)(T - 1) * n, n, a.cand_idx, kp, nn, oi,
+                         od, s));
+  c->launches += 1;
   DRPT_CUDA(cudaEventRecord(ev[5], s));
   int err = 0;
   DRPT_CUDA(cudaMemcpyAsync(&err, a.err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -430,6 +433,17 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
         mx = std::max<int>(mx, (int)m);
       }
     stats->sum_leaf_sq = sq;
+    int64_t padded = 0;  // 128 x 64 tiles over every leaf
+    for (int t = 0; t < T; ++t)
+      for (int j = 0; j < nleaf; ++j) {
+        const int64_t m = h[(size_t)t * (nleaf + 1) + j + 1] - h[(size_t)t * (nleaf + 1) + j];
+        padded += ceil_div(m, 128) * 128 * ceil_div(m, 64) * 64;
+      }
+    stats->mma_pairs_padded = padded;
+    for (int t = 0; t < T; ++t) {
+      stats->ms_leaf_stage += elapsed(c->tev[3 * t], c->tev[3 * t + 1]);
+      stats->ms_leaf_mma += elapsed(c->tev[3 * t + 1], c->tev[3 * t + 2]);
+    }
     stats->min_global_leaf = mn;
     stats->max_final_leaf = mx;
     stats->kernels_launched = c->launches - launches0;
@@ -483,6 +497,8 @@ void drpt_ctx_destroy(drpt_ctx *c) {
   for (auto &kv : c->bufs)
     if (kv.second.p) cudaFree(kv.second.p);
   for (auto &e : c->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto &e : c->tev)
     if (e) cudaEventDestroy(e);
   delete c;
 }

@@ -12,9 +12,12 @@
 //                       FP32 in Tensor Memory, M = 128 rows, N = 64 columns
 //                       per tile, K = the padded dimension), epilogue scores
 //                       ||y||^2 - 2 x.y per column and keeps each row's KP
-//                       best in registers (threshold filter, per-thread
-//                       shared-memory buffer, lock-step flushes)
-//   K11 k_rerank        per point: the merged 2k candidates rescored with the
+//                       best in registers (threshold filter seeded from the
+//                       running list, per-thread shared-memory buffer,
+//                       bitonic sort + merge), then folds them into the
+//                       point's running list of the KP best distinct
+//                       candidates over the trees built so far
+//   K11 k_rerank        per point: the running list's KP candidates rescored with the
 //                       exact sequential FP32 distance of the plain form, the
 //                       k best kept; candidates whose FP32 distance lies within
 //                       a relative 2^-16 of the k-th are re-ordered by an FP64
@@ -24,6 +27,9 @@
 // to the squared distances that are ranked (values of a few tens instead of a
 // few hundreds for the synthetic workloads).
 #include <cuda.h>
+
+#include <algorithm>
+#include <type_traits>
 
 #include "kernels.cuh"
 #include "sm100.cuh"
@@ -40,6 +46,7 @@ constexpr int kBufCap = 32;         // per-row pending candidates
 constexpr int kCheck = 16;          // columns between flush checks
 constexpr int kEpiWarps = 4;
 constexpr int kMmaThreads = 32 * (kEpiWarps + 2);
+constexpr int kCentreRows = 64;     // rows averaged for a leaf's centre
 
 __device__ __forceinline__ bool before(float da, int32_t ia, float db, int32_t ib) {
   return da < db || (da == db && (uint32_t)ia < (uint32_t)ib);
@@ -61,8 +68,9 @@ __device__ __forceinline__ void load4<uint8_t>(const uint8_t *p, float *v) {
 
 // One block per global leaf.  Warps take rows in turn; lane l owns the four
 // dimensions 4l..4l+3 of every 128-wide chunk (d <= 256, d % 4 == 0).  The
-// leaf mean is summed per warp and the eight warp partials are added in
-// warp order, so the result does not depend on scheduling.
+// centre is the mean of the leaf's first (up to) kCentreRows rows -- it only
+// has to bring the values near zero -- summed per warp, the eight warp
+// partials added in warp order, so the result does not depend on scheduling.
 template <typename T>
 __global__ void __launch_bounds__(256) k_leaf_center(const T *__restrict__ X, int d, int d_pad,
                                                      const int32_t *__restrict__ order,
@@ -76,7 +84,8 @@ __global__ void __launch_bounds__(256) k_leaf_center(const T *__restrict__ X, in
   const int m = hi - lo;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
-  for (int r = warp; r < m; r += 8) {
+  const int mc = min(m, kCentreRows);
+  for (int r = warp; r < mc; r += 8) {
     const T *src = X + (int64_t)__ldg(order + lo + r) * d;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -97,32 +106,46 @@ __global__ void __launch_bounds__(256) k_leaf_center(const T *__restrict__ X, in
   if (threadIdx.x < 256) {
     float s = 0.0f;
     for (int w = 0; w < 8; ++w) s += part[w][threadIdx.x];
-    mu[threadIdx.x] = m > 0 ? s / (float)m : 0.0f;
+    mu[threadIdx.x] = mc > 0 ? s / (float)mc : 0.0f;
   }
   __syncthreads();
-  for (int r = warp; r < m; r += 8) {
-    const T *src = X + (int64_t)__ldg(order + lo + r) * d;
-    __nv_bfloat16 *dst = Xb + (int64_t)(lo + r) * d_pad;
-    float sq = 0.0f;
+  constexpr int RB = 4;  // rows per warp step, loaded together
+  for (int r0w = warp * RB; r0w < m; r0w += 8 * RB) {
+    float v[RB][2][4];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int c0 = h * 128 + 4 * lane;
-      if (c0 < d_pad) {
-        float v[4] = {0.f, 0.f, 0.f, 0.f};
-        if (c0 < d) load4<T>(src + c0, v);
-        __nv_bfloat16 b[4];
+    for (int q = 0; q < RB; ++q) {
+      const int r = r0w + q;
+      const T *src = r < m ? X + (int64_t)__ldg(order + lo + r) * d : nullptr;
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          b[e] = __float2bfloat16_rn(c0 + e < d ? v[e] - mu[c0 + e] : 0.0f);
-          const float vr = __bfloat162float(b[e]);
-          sq = fmaf(vr, vr, sq);
-        }
-        *reinterpret_cast<uint2 *>(dst + c0) = *reinterpret_cast<const uint2 *>(b);
+      for (int h = 0; h < 2; ++h) {
+        const int c0 = h * 128 + 4 * lane;
+        v[q][h][0] = v[q][h][1] = v[q][h][2] = v[q][h][3] = 0.0f;
+        if (src && c0 < d) load4<T>(src + c0, v[q][h]);
       }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(kFull, sq, o);
-    if (lane == 0) nrm[lo + r] = sq;
+    for (int q = 0; q < RB; ++q) {
+      const int r = r0w + q;
+      float sq = 0.0f;
+      __nv_bfloat16 *dst = Xb + (int64_t)(lo + (r < m ? r : 0)) * d_pad;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c0 = h * 128 + 4 * lane;
+        if (c0 < d_pad) {
+          __nv_bfloat16 b[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            b[e] = __float2bfloat16_rn(c0 + e < d ? v[q][h][e] - mu[c0 + e] : 0.0f);
+            const float vr = __bfloat162float(b[e]);
+            sq = fmaf(vr, vr, sq);
+          }
+          if (r < m) *reinterpret_cast<uint2 *>(dst + c0) = *reinterpret_cast<const uint2 *>(b);
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(kFull, sq, o);
+      if (lane == 0 && r < m) nrm[lo + r] = sq;
+    }
   }
 }
 
@@ -222,16 +245,16 @@ __device__ __forceinline__ void bitonic_merge_into(float *L, int32_t *Li, const 
 }
 
 struct MmaSmem {
-  uint32_t a_off, b_off, bufd_off, bufi_off, bar_off, total;
+  uint32_t a_off, b_off, buf_off, nrm_off, bar_off, total;
 };
 
 __host__ __device__ inline MmaSmem mma_smem_layout(int kb) {
   MmaSmem L;
   L.a_off = 0;
   L.b_off = L.a_off + (uint32_t)kb * kTM * 128;
-  L.bufd_off = L.b_off + (uint32_t)kStages * kb * kTN * 128;
-  L.bufi_off = L.bufd_off + kTM * kBufCap * 4;
-  L.bar_off = L.bufi_off + kTM * kBufCap * 4;
+  L.buf_off = L.b_off + (uint32_t)kStages * kb * kTN * 128;
+  L.nrm_off = L.buf_off + kTM * kBufCap * 8;
+  L.bar_off = L.nrm_off + kEpiWarps * kTN * 4;
   L.total = L.bar_off + 16 * 8 + 16;
   return L;
 }
@@ -241,16 +264,16 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
     const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
     const int32_t *__restrict__ goff, const int32_t *__restrict__ order,
     const float *__restrict__ nrm, const int32_t *__restrict__ tile_leaf,
-    const int32_t *__restrict__ tile_r0, const int32_t *__restrict__ n_tiles, int kb, int T,
-    int tree, int32_t *__restrict__ cand_idx, float *__restrict__ cand_dist, int *err) {
+    const int32_t *__restrict__ tile_r0, const int32_t *__restrict__ n_tiles, int kb, int tree,
+    int32_t *__restrict__ run_idx, float *__restrict__ run_dist, int *err) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
   const MmaSmem L = mma_smem_layout(kb);
   uint8_t *sA = smem + L.a_off;
   uint8_t *sB = smem + L.b_off;
-  float *bufd = reinterpret_cast<float *>(smem + L.bufd_off);
-  int32_t *bufi = reinterpret_cast<int32_t *>(smem + L.bufi_off);
+  uint2 *buf = reinterpret_cast<uint2 *>(smem + L.buf_off);  // [slot][row]: (value bits, position)
+  float *nbuf = reinterpret_cast<float *>(smem + L.nrm_off);  // [warp][kTN] column norms of a tile
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L.bar_off);
   uint64_t *full_a = bars + 0;
   uint64_t *full_b = bars + 1;             // kStages
@@ -339,7 +362,6 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
     // and merges them into its sorted list with a bitonic network.
     const int row = warp * 32 + lane;
     const bool rvalid = r0 + row < m;
-    const int my_col = r0 + row;
     float td[KP];
     int32_t ti[KP];
 #pragma unroll
@@ -347,9 +369,28 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
       td[j] = __int_as_float(0x7f800000);
       ti[j] = -1;
     }
-    float thr = __int_as_float(0x7f800000);
-    int cnt = 0;
+    // Candidates that cannot beat the KP-th of the point's running list
+    // (approximate squared distances of the earlier trees) are never kept.
+    // (rows past the leaf get -inf and keep nothing)
+    float thr = rvalid ? __int_as_float(0x7f800000) : -__int_as_float(0x7f800000);
+    int32_t my_pos = -1, my_pt = -1;
+    float nr = 0.0f;
+    if (rvalid) {
+      my_pos = lo + r0 + row;
+      my_pt = __ldg(order + my_pos);
+      nr = __ldg(nrm + my_pos);
+      if (tree > 0) thr = run_dist[(int64_t)my_pt * KP + KP - 1] - nr;
+    }
+    const float thr0 = thr;
+    // Pending candidates: a passing candidate is stored at the row's next
+    // free slot by a predicated shared-memory store (no branch); slot
+    // addresses are 32-bit shared-window offsets.
+    uint2 *const pbase = buf + row;
+    const uint32_t abase = smem_u32(pbase);
+    uint32_t aslot = abase;
+    auto pending = [&]() { return (int)((aslot - abase) / (kTM * 8)); };
     auto flush = [&]() {
+      const int cnt = pending();
       const int mx = __reduce_max_sync(kFull, cnt);
       for (int base = 0; base < mx; base += 16) {
         float sd[16];
@@ -358,14 +399,44 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
         for (int e = 0; e < 16; ++e) {
           const int slot = base + e;
           const bool have = slot < cnt;
-          sd[e] = have ? bufd[slot * kTM + row] : __int_as_float(0x7f800000);
-          si[e] = have ? bufi[slot * kTM + row] : -1;
+          const uint2 ent = have ? pbase[slot * kTM] : make_uint2(0x7f800000u, 0xffffffffu);
+          sd[e] = __uint_as_float(ent.x);
+          si[e] = (int32_t)ent.y;
         }
         bitonic_sort<16>(sd, si);
         bitonic_merge_into<KP, 16>(td, ti, sd, si);
       }
-      cnt = 0;
-      thr = td[KP - 1];
+      aslot = abase;
+      thr = fminf(thr0, td[KP - 1]);
+    };
+    // one 32-column chunk of scores; DIAG: the warp's diagonal chunk, where
+    // lane l's own point is column l and is skipped
+    auto scan = [&](const float *v, const float *wn, int cb, auto diag_tag) {
+      constexpr bool DIAG = decltype(diag_tag)::value;
+#pragma unroll
+      for (int h = 0; h < 32; h += kCheck) {
+#pragma unroll
+        for (int j4 = h; j4 < h + kCheck; j4 += 4) {
+          const float4 nc4 = *reinterpret_cast<const float4 *>(wn + j4);
+          const float ncs[4] = {nc4.x, nc4.y, nc4.z, nc4.w};
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int j = j4 + e;
+            float sv = fmaf(-2.0f, v[j], ncs[e]);
+            if (DIAG) sv = (j == lane) ? __int_as_float(0x7f800000) : sv;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.lt.f32 p, %1, %2;\n\t"
+                "@p st.shared.v2.u32 [%0], {%3, %4};\n\t"
+                "@p add.u32 %0, %0, %5;\n\t}"
+                : "+r"(aslot)
+                : "f"(sv), "f"(thr), "r"(__float_as_uint(sv)), "r"((uint32_t)(cb + j)),
+                  "n"(kTM * 8)
+                : "memory");
+          }
+        }
+        if (__any_sync(kFull, pending() >= kBufCap - kCheck)) flush();
+      }
     };
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
     for (int c = 0; c < nct; ++c) {
@@ -375,42 +446,57 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
         break;
       }
       tc_fence_after();
+      // this tile's column norms, staged per warp (16-byte aligned reads);
+      // columns past the leaf carry an infinite norm and so never pass
+      float *wn = nbuf + warp * kTN;
+      __syncwarp();
+#pragma unroll
+      for (int h = 0; h < kTN; h += 32) {
+        const int col = c * kTN + h + lane;
+        wn[h + lane] = col < m ? __ldg(nrm + lo + col) : __int_as_float(0x7f800000);
+      }
+      __syncwarp();
 #pragma unroll
       for (int q = 0; q < kTN / 32; ++q) {
         float v[32];
         tmem_ld32(lane_base + b * kTN + q * 32, v);
         const int cb = c * kTN + q * 32;
-        const float ncv = cb + lane < m ? __ldg(nrm + lo + cb + lane) : 0.0f;
-        const int lim = rvalid ? min(32, m - cb) : 0;  // valid columns of this chunk
-#pragma unroll
-        for (int h = 0; h < 32; h += kCheck) {
-#pragma unroll
-          for (int j = h; j < h + kCheck; ++j) {
-            const float nc = __shfl_sync(kFull, ncv, j);
-            const float sv = fmaf(-2.0f, v[j], nc);
-            if (j < lim && cb + j != my_col && sv < thr) {
-              bufd[cnt * kTM + row] = sv;
-              bufi[cnt * kTM + row] = lo + cb + j;
-              ++cnt;
-            }
-          }
-          if (__any_sync(kFull, cnt >= kBufCap - kCheck)) flush();
-        }
+        // the warp's 32 rows sit in one 32-column chunk of the diagonal
+        if (cb == r0 + warp * 32)
+          scan(v, wn + q * 32, lo + cb, std::true_type{});
+        else
+          scan(v, wn + q * 32, lo + cb, std::false_type{});
       }
       tc_fence_before();
       mbar_arrive(acc_empty + b);
     }
     flush();
     if (rvalid) {
-      const int32_t pos = lo + r0 + row;
-      const int32_t p = __ldg(order + pos);
-      const float nr = __ldg(nrm + pos);
-      const int64_t o = ((int64_t)p * T + tree) * KP;
+      // fold this tree's list into the running list: drop neighbours it
+      // already holds, then a bitonic merge keeps the KP best
+      const int64_t o = (int64_t)my_pt * KP;
+      float rd[KP];
+      int32_t ri[KP];
 #pragma unroll
       for (int j = 0; j < KP; ++j) {
-        const bool have = ti[j] >= 0;
-        cand_idx[o + j] = have ? __ldg(order + ti[j]) : -1;
-        cand_dist[o + j] = have ? nr + td[j] : __int_as_float(0x7f800000);
+        rd[j] = tree > 0 ? run_dist[o + j] : __int_as_float(0x7f800000);
+        ri[j] = tree > 0 ? run_idx[o + j] : -1;
+      }
+#pragma unroll
+      for (int j = 0; j < KP; ++j) {
+        int32_t q = ti[j] >= 0 ? __ldg(order + ti[j]) : -1;
+        bool dup = false;
+#pragma unroll
+        for (int i = 0; i < KP; ++i) dup |= (q >= 0 && ri[i] == q);
+        ti[j] = dup ? -1 : q;
+        td[j] = (dup || q < 0) ? __int_as_float(0x7f800000) : nr + td[j];
+      }
+      bitonic_sort<KP>(td, ti);
+      bitonic_merge_into<KP, KP>(rd, ri, td, ti);
+#pragma unroll
+      for (int j = 0; j < KP; ++j) {
+        run_dist[o + j] = rd[j];
+        run_idx[o + j] = ri[j];
       }
     }
   }
@@ -424,49 +510,66 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
 }
 
 // ------------------------------------------------------------------ K11
-template <typename T>
-__device__ __forceinline__ float row_elem(const T *X, int64_t i) { return (float)X[i]; }
+// One warp per point.  The warp stages the query row and its K2 candidate
+// rows in shared memory with coalesced loads (rows padded to d + 4 floats so
+// that the float4 reads below hit distinct banks), then lane j computes the
+// exact FP32 distance of candidate j: the sequential sum, in dimension order,
+// of rounded squares of rounded differences, and its rounded square root.
+// d must be a multiple of 4.
+template <typename T, int D>
+__device__ __forceinline__ float exact_dist(const T *__restrict__ xp, const T *__restrict__ xc,
+                                            int d) {
+  // sequential FP32 sum over the dimensions in order (D > 0: compile-time d);
+  // rows are read four values at a time straight from global memory
+  float s = 0.0f;
+  const int dd = D > 0 ? D : d;
+#pragma unroll(D > 0 ? D / 4 : 4)
+  for (int i = 0; i < dd; i += 4) {
+    float a[4], b[4];
+    load4<T>(xp + i, a);
+    load4<T>(xc + i, b);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const float df = __fsub_rn(b[e], a[e]);
+      s = __fadd_rn(s, __fmul_rn(df, df));
+    }
+  }
+  return __fsqrt_rn(s);
+}
 
-// d must be a multiple of 4 (rows are read four values at a time, in order).
-template <typename T>
+// G = 32 / K2 points per warp; lanes [g*K2, (g+1)*K2) serve point g, lane
+// j of a group computes candidate j from the two rows in global memory (the
+// query row is the same address for the whole group).  The K2 (distance,
+// index) pairs are then sorted with a bitonic network inside the group and
+// the first k kept; candidates whose FP32 distance lies within 2^-16 of the
+// k-th are re-ordered by an FP64 distance.  d must be a multiple of 4.
+template <typename T, int D, int K2>
 __global__ void __launch_bounds__(256) k_rerank(const T *__restrict__ X, int d,
                                                 const int32_t *__restrict__ visit, int64_t n,
-                                                const int32_t *__restrict__ ci, int K2, int k,
+                                                const int32_t *__restrict__ ci, int k,
                                                 int32_t *__restrict__ oi, float *__restrict__ od) {
+  constexpr int G = 32 / K2;
   const int lane = threadIdx.x & 31;
-  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (w >= n) return;
-  const int32_t p = visit ? __ldg(visit + w) : (int32_t)w;
+  const int g = lane / K2, j = lane % K2;
+  const int64_t wglob = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t w = wglob * G + g;       // this lane's point slot
+  if (wglob * G >= n) return;            // warp-uniform
+  const bool live = w < n;
+  const int32_t p = live ? (visit ? __ldg(visit + w) : (int32_t)w) : -1;
   const float inf = __int_as_float(0x7f800000);
-  const int32_t c = lane < K2 ? __ldg(ci + (int64_t)p * K2 + lane) : -1;
+  const int32_t c = live ? __ldg(ci + (int64_t)p * K2 + j) : -1;
   float dist = inf;
-  if (c >= 0) {
-    // exact FP32 distance: sequential sum of rounded squares of rounded differences
-    const T *xp = X + (int64_t)p * d, *xc = X + (int64_t)c * d;
-    float s = 0.0f;
-#pragma unroll 8
-    for (int i = 0; i < d; i += 4) {
-      float a[4], b[4];
-      load4<T>(xp + i, a);
-      load4<T>(xc + i, b);
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const float df = __fsub_rn(b[e], a[e]);
-        s = __fadd_rn(s, __fmul_rn(df, df));
-      }
-    }
-    dist = __fsqrt_rn(s);
-  }
+  if (c >= 0) dist = exact_dist<T, D>(X + (int64_t)p * d, X + (int64_t)c * d, d);
   int32_t id = c;
-  // bitonic sort of 32 (dist, id) pairs across the warp, ascending
+  // bitonic sort of K2 (dist, id) pairs inside the group, ascending
 #pragma unroll
-  for (int size = 2; size <= 32; size <<= 1) {
+  for (int size = 2; size <= K2; size <<= 1) {
 #pragma unroll
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
       const float od_ = __shfl_xor_sync(kFull, dist, stride);
       const int32_t oi_ = __shfl_xor_sync(kFull, id, stride);
-      const bool up = ((lane & size) == 0);
-      const bool lower = (lane & stride) == 0;
+      const bool up = ((j & size) == 0);
+      const bool lower = (j & stride) == 0;
       const bool mine_first = before(dist, id, od_, oi_);
       const bool keep = (lower == up) ? mine_first : !mine_first;
       if (!keep) {
@@ -476,39 +579,42 @@ __global__ void __launch_bounds__(256) k_rerank(const T *__restrict__ X, int d,
     }
   }
   // FP64 check of the candidates near the k-th distance
-  const float dk = __shfl_sync(kFull, dist, k - 1);
+  const float dk = __shfl_sync(kFull, dist, g * K2 + k - 1);
   const float eps = 1.52587890625e-05f;  // 2^-16
   const bool near = id >= 0 && isfinite(dk) && fabsf(dist - dk) <= eps * dk;
-  if (__any_sync(kFull, near && lane >= k) && __any_sync(kFull, near && lane < k)) {
+  const unsigned gmask = (K2 == 32 ? 0xffffffffu : ((1u << K2) - 1u)) << (g * K2);
+  const unsigned wmask = __ballot_sync(kFull, near) & gmask;
+  const unsigned below = gmask & ((1u << (g * K2 + k)) - 1u);
+  if (__any_sync(kFull, (wmask & below) != 0 && (wmask & ~below) != 0)) {
+    const bool act = (wmask & below) != 0 && (wmask & ~below) != 0;  // group-uniform
     double d64 = 1e300;
-    if (near) {
+    if (act && near) {
       const T *xp = X + (int64_t)p * d, *xc = X + (int64_t)id * d;
       double s = 0.0;
       for (int i = 0; i < d; ++i) {
-        const double df = (double)row_elem(xc, i) - (double)row_elem(xp, i);
+        const double df = (double)xc[i] - (double)xp[i];
         s += df * df;
       }
       d64 = sqrt(s);
     }
-    // re-order the window by (FP64 distance, id); lanes outside keep their place
-    const unsigned wmask = __ballot_sync(kFull, near);
-    const int first = __ffs(wmask) - 1;
+    // re-order the window by (FP64 distance, id); other lanes keep their place
+    const int first = act ? __ffs(wmask) - 1 : lane;
     int rank = 0;
-    for (int j = 0; j < 32; ++j) {
-      if (!((wmask >> j) & 1u)) continue;
-      const double oj = __shfl_sync(kFull, d64, j);
-      const int32_t ij = __shfl_sync(kFull, id, j);
-      if (near && (oj < d64 || (oj == d64 && (uint32_t)ij < (uint32_t)id))) ++rank;
+    for (int q = 0; q < 32; ++q) {
+      const double oq = __shfl_sync(kFull, d64, q);
+      const int32_t iq = __shfl_sync(kFull, id, q);
+      if (act && near && ((wmask >> q) & 1u) &&
+          (oq < d64 || (oq == d64 && (uint32_t)iq < (uint32_t)id)))
+        ++rank;
     }
-    const int dest = first + rank;
+    const int dest = (act && near) ? first + rank : lane;
     float nd = dist;
     int32_t ni = id;
-    // lane `dest` receives the entry that ranks there
-    for (int j = 0; j < 32; ++j) {
-      const int dj = __shfl_sync(kFull, dest, j);
-      const float dv = __shfl_sync(kFull, dist, j);
-      const int32_t iv = __shfl_sync(kFull, id, j);
-      if (((wmask >> j) & 1u) && dj == lane) {
+    for (int q = 0; q < 32; ++q) {
+      const int dq = __shfl_sync(kFull, dest, q);
+      const float dv = __shfl_sync(kFull, dist, q);
+      const int32_t iv = __shfl_sync(kFull, id, q);
+      if (act && ((wmask >> q) & 1u) && dq == lane) {
         nd = dv;
         ni = iv;
       }
@@ -516,9 +622,33 @@ __global__ void __launch_bounds__(256) k_rerank(const T *__restrict__ X, int d,
     dist = nd;
     id = ni;
   }
-  if (lane < k) {
-    oi[(int64_t)p * k + lane] = id;
-    od[(int64_t)p * k + lane] = id >= 0 ? dist : inf;
+  if (live && j < k) {
+    oi[(int64_t)p * k + j] = id;
+    od[(int64_t)p * k + j] = id >= 0 ? dist : inf;
+  }
+}
+
+template <typename T, int D, int K2>
+drpt_status launch_rerank_t(const void *X, int d, const int32_t *visit, int64_t n,
+                            const int32_t *cand, int k, int32_t *out_idx, float *out_dist,
+                            cudaStream_t s) {
+  constexpr int G = 32 / K2;
+  const int64_t warps = ceil_div(n, G);
+  const unsigned grid = (unsigned)ceil_div(warps * 32, 256);
+  k_rerank<T, D, K2><<<grid, 256, 0, s>>>((const T *)X, d, visit, n, cand, k, out_idx, out_dist);
+  DRPT_LAUNCH_CHECK();
+  return DRPT_OK;
+}
+
+template <typename T, int K2>
+drpt_status launch_rerank_d(const void *X, int d, const int32_t *visit, int64_t n,
+                            const int32_t *cand, int k, int32_t *out_idx, float *out_dist,
+                            cudaStream_t s) {
+  switch (d) {
+    case 128: return launch_rerank_t<T, 128, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
+    case 96: return launch_rerank_t<T, 96, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
+    case 256: return launch_rerank_t<T, 256, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
+    default: return launch_rerank_t<T, 0, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
   }
 }
 
@@ -596,14 +726,14 @@ drpt_status launch_leaf_mma(const MixedTreeArgs &a, cudaStream_t s) {
     DRPT_CUDA(cudaFuncSetAttribute(k_leaf_mma<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
     k_leaf_mma<16><<<grid, kMmaThreads, smem, s>>>(tmA, tmB, a.goff, a.order, a.nrm, a.tile_leaf,
-                                                   a.tile_r0, a.n_tiles, kb, a.T, a.tree,
-                                                   a.cand_idx, a.cand_dist, a.err);
+                                                   a.tile_r0, a.n_tiles, kb, a.tree, a.cand_idx,
+                                                   a.cand_dist, a.err);
   } else if (a.kp == 32) {
     DRPT_CUDA(cudaFuncSetAttribute(k_leaf_mma<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
     k_leaf_mma<32><<<grid, kMmaThreads, smem, s>>>(tmA, tmB, a.goff, a.order, a.nrm, a.tile_leaf,
-                                                   a.tile_r0, a.n_tiles, kb, a.T, a.tree,
-                                                   a.cand_idx, a.cand_dist, a.err);
+                                                   a.tile_r0, a.n_tiles, kb, a.tree, a.cand_idx,
+                                                   a.cand_dist, a.err);
   } else {
     set_error("mixed leaf kernel: %d candidates per tree unsupported (16 or 32)", a.kp);
     return DRPT_ERR_UNSUPPORTED;
@@ -615,19 +745,19 @@ drpt_status launch_leaf_mma(const MixedTreeArgs &a, cudaStream_t s) {
 drpt_status launch_rerank(const void *X, int dtype, int d, const int32_t *visit, int64_t n,
                           const int32_t *cand, int K2, int k, int32_t *out_idx, float *out_dist,
                           cudaStream_t s) {
-  if (K2 > 32 || k > K2 || k <= 0) {
-    set_error("re-rank: %d candidates for k = %d unsupported (at most 32)", K2, k);
+  if ((K2 != 16 && K2 != 32) || k > K2 || k <= 0) {
+    set_error("re-rank: %d candidates for k = %d unsupported (16 or 32)", K2, k);
     return DRPT_ERR_UNSUPPORTED;
   }
-  const unsigned grid = (unsigned)ceil_div(n * 32, 256);
+  if (d % 4 != 0) {
+    set_error("re-rank needs d %% 4 == 0 (got %d)", d);
+    return DRPT_ERR_UNSUPPORTED;
+  }
   if (dtype == DRPT_DTYPE_U8)
-    k_rerank<uint8_t><<<grid, 256, 0, s>>>((const uint8_t *)X, d, visit, n, cand, K2, k, out_idx,
-                                            out_dist);
-  else
-    k_rerank<float><<<grid, 256, 0, s>>>((const float *)X, d, visit, n, cand, K2, k, out_idx,
-                                          out_dist);
-  DRPT_LAUNCH_CHECK();
-  return DRPT_OK;
+    return K2 == 16 ? launch_rerank_d<uint8_t, 16>(X, d, visit, n, cand, k, out_idx, out_dist, s)
+                    : launch_rerank_d<uint8_t, 32>(X, d, visit, n, cand, k, out_idx, out_dist, s);
+  return K2 == 16 ? launch_rerank_d<float, 16>(X, d, visit, n, cand, k, out_idx, out_dist, s)
+                  : launch_rerank_d<float, 32>(X, d, visit, n, cand, k, out_idx, out_dist, s);
 }
 
 }  // namespace drpt

@@ -92,12 +92,12 @@ struct MixedTreeArgs {
   const int32_t *order;      // this tree's global-leaf order (n)
   const int32_t *goff;       // this tree's leaf starts (nleaf + 1)
   int nleaf;
-  int T, tree, kp;           // trees, this tree, candidates kept per tree
+  int T, tree, kp;           // trees, this tree, candidates kept per point
   __nv_bfloat16 *Xb;         // n x d_pad, centred rows in leaf order
   float *nrm;                // n, squared norms of the BF16 rows
   int32_t *tile_leaf, *tile_r0, *n_tiles;  // n / 128 + nleaf
-  int32_t *cand_idx;         // n x T x kp
-  float *cand_dist;          // n x T x kp (approximate squared distances)
+  int32_t *cand_idx;         // n x kp running list (point ids), updated tree by tree
+  float *cand_dist;          // n x kp approximate squared distances, ascending
   int *err;                  // set when a bounded wait gave up
 };
 drpt_status launch_leaf_center(const MixedTreeArgs &a, cudaStream_t s);

@@ -105,6 +105,10 @@ typedef struct {
   int32_t kernels_launched;   /* device kernels this call launched */
   int32_t reserved;
   float ms_project, ms_global, ms_local, ms_leaf_knn, ms_merge, ms_total;
+  /* mixed mode: time of the tensor-core leaf kernels alone (all trees) and
+   * of the BF16 staging kernels; padded Gram-tile multiply-adds per call */
+  float ms_leaf_mma, ms_leaf_stage;
+  int64_t mma_pairs_padded;
 } drpt_stats;
 
 /* Library version string. */

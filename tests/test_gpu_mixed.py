@@ -1,0 +1,89 @@
+"""The mixed-precision form (BF16 tcgen05 leaf tiles, FP32 re-rank, FP64
+boundary check): recall against FP64 exact neighbours, exact FP32 output
+distances, determinism and its stated limits.  Needs a B200."""
+import numpy as np
+import pytest
+
+import oracle
+from drpt_b200 import DrptError, build_graph, recall, synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as _t
+    if not _t.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return _t
+
+
+def _exact_fp32(a, b):
+    return oracle.distance(a.astype(np.float32), b.astype(np.float32))
+
+
+@pytest.fixture(scope="module")
+def clustered(torch):
+    X = synth.clustered_f32(120_000, 128, n_clusters=120, seed=41)
+    return X, torch.from_numpy(X).cuda()
+
+
+def test_mixed_recall_and_exact_distances(torch, clustered):
+    X, Xd = clustered
+    idx, dist, st = build_graph(Xd, 6, 10, 99, mode="mixed", leaf_size=1024)
+    torch.cuda.synchronize()
+    I, D = idx.cpu().numpy(), dist.cpu().numpy()
+    q = recall.sample_queries(len(X), 400, seed=3)
+    ti, _ = recall.exact_knn_fp64(Xd, q, 10)
+    r = recall.recall_at_k(I[q], ti)
+    assert r >= 0.85, r
+    assert not (I == np.arange(len(X))[:, None]).any()
+    assert (I >= 0).all()
+    assert ((D[:, 1:] >= D[:, :-1])).all()
+    for p in q[:25]:
+        assert len(np.unique(I[p])) == I.shape[1]
+        for j in range(0, 10, 3):
+            assert D[p, j] == _exact_fp32(X[p], X[I[p, j]])
+
+
+def test_mixed_is_deterministic(torch, clustered):
+    _, Xd = clustered
+    a = build_graph(Xd, 4, 10, 5, mode="mixed", leaf_size=512)
+    b = build_graph(Xd, 4, 10, 5, mode="mixed", leaf_size=512)
+    torch.cuda.synchronize()
+    assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
+
+
+def test_mixed_recall_grows_with_trees(torch, clustered):
+    X, Xd = clustered
+    q = recall.sample_queries(len(X), 300, seed=4)
+    ti, _ = recall.exact_knn_fp64(Xd, q, 10)
+    rs = []
+    for T in (1, 3, 6):
+        idx, _, _ = build_graph(Xd, T, 10, 11, mode="mixed", leaf_size=1024)
+        rs.append(recall.recall_at_k(idx.cpu().numpy()[q], ti))
+    assert rs[0] < rs[1] <= rs[2] + 1e-9, rs
+
+
+def test_mixed_u8_and_k16(torch):
+    X = synth.clustered_u8(30_000, 784 // 7 * 2, seed=8)  # 224 dims, u8
+    Xd = torch.from_numpy(X).cuda()
+    idx, dist, _ = build_graph(Xd, 4, 16, 3, mode="mixed", leaf_size=1024)
+    torch.cuda.synchronize()
+    I, D = idx.cpu().numpy(), dist.cpu().numpy()
+    for p in (0, 17, 2999):
+        assert D[p, 0] == _exact_fp32(X[p], X[I[p, 0]])
+    q = recall.sample_queries(len(X), 200, seed=5)
+    ti, _ = recall.exact_knn_fp64(Xd, q, 16)
+    assert recall.recall_at_k(I[q], ti) > 0.5
+
+
+def test_mixed_limits_are_reported(torch):
+    X = np.random.default_rng(0).random((5000, 960), dtype=np.float32)
+    with pytest.raises(DrptError) as e:
+        build_graph(X, 2, 10, 1, mode="mixed")
+    assert e.value.status == 8
+    X = np.random.default_rng(0).random((5000, 64), dtype=np.float32)
+    with pytest.raises(DrptError) as e:
+        build_graph(X, 2, 20, 1, mode="mixed")
+    assert e.value.status == 8
