@@ -47,7 +47,7 @@ sys.path.insert(0, ROOT)
 METRIC = "kNN-graph points/s at recall@10≥0.90, mixed/learned vs plain FP32, 1 B200"
 N_POINTS, DIM, NTREES, NN, N_CLUSTERS = 1_000_000, 128, 16, 10, 1000
 MIXED_TREES, MIXED_LEAF = 6, 1024   # mixed form: trees and target global-leaf size
-PLAIN_MATCH_TREES = 384             # plain form grown towards the mixed form's recall
+PLAIN_MATCH_TREES = 384             # the reference method with many more trees
 SEED_PROJ = 12345
 CPU_SAMPLE = 32_768  # bounded sample for the CPU baseline (about 10-30 s of CPU work)
 REF_STEP_SAMPLE = 16_384  # per timed step of --impl reference
@@ -332,30 +332,36 @@ def main():
                "d2h_bytes_per_step": int(oi.numel() * 4 + od.numel() * 4)}
 
     # the plain FP32 form beside it (one GPU only): reference parameters, and
-    # grown towards the mixed form's recall
+    # grown towards the mixed form's recall, and the FP32 counterpart of the
+    # mixed form (same trees, exact FP32 leaf brute force)
     plain = None
     if not args.no_plain_compare and world == 1 and args.mode == "mixed":
         plain = {}
-        for name, mode, ntrees in (("exact_16_trees", "exact", NTREES),
-                                   ("fast_16_trees", "fast", NTREES),
-                                   (f"fast_{PLAIN_MATCH_TREES}_trees", "fast", PLAIN_MATCH_TREES)):
+        for name, mode, ntrees, lsz in (
+                ("exact_16_trees", "exact", NTREES, 0),
+                ("fast_16_trees", "fast", NTREES, 0),
+                (f"fast_{PLAIN_MATCH_TREES}_trees", "fast", PLAIN_MATCH_TREES, 0),
+                (f"fp32_leaf_{MIXED_TREES}_trees", "fp32_leaf", MIXED_TREES, MIXED_LEAF)):
             pi = torch.empty((N_POINTS, NN), dtype=torch.int32, device=dev)
             pd = torch.empty((N_POINTS, NN), dtype=torch.float32, device=dev)
-            step(mode, ntrees, 0, Xd, (pi, pd))
+            step(mode, ntrees, lsz, Xd, (pi, pd))
             torch.cuda.synchronize()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            step(mode, ntrees, 0, Xd, (pi, pd))
+            step(mode, ntrees, lsz, Xd, (pi, pd))
             b.record(stream)
             torch.cuda.synchronize()
             pms = a.elapsed_time(b)
             plain[name] = {"points_per_s": N_POINTS / (pms / 1e3), "ms": pms, "ntrees": ntrees,
                            "recall@10": recall.recall_at_k(pi.cpu().numpy()[q], true_i)}
             del pi, pd
-        best_plain = max(v["points_per_s"] for v in plain.values() if v["recall@10"] >= rec - 0.02) \
-            if any(v["recall@10"] >= rec - 0.02 for v in plain.values()) else None
-        plain["mixed_over_plain_at_equal_recall"] = (world * N_POINTS / (ms / 1e3)) / best_plain \
-            if best_plain else None
+        # Equal recall: only the FP32 whole-leaf form (same trees and leaves as
+        # the mixed form) reaches it; the reference's positional local split
+        # saturates far below (see fast_{PLAIN_MATCH_TREES}_trees).
+        eq = [v for v in plain.values() if v["recall@10"] >= rec - 0.01]
+        best_plain = max(v["points_per_s"] for v in eq) if eq else None
+        plain["mixed_over_plain_fp32_at_equal_recall"] = \
+            (world * N_POINTS / (ms / 1e3)) / best_plain if best_plain else None
 
     if rank != 0:
         if world > 1:

@@ -306,7 +306,7 @@ drpt_status check_common(const drpt_build_desc *d) {
   if (!d) return DRPT_ERR_INVALID_ARG;
   if (d->n < 2 || d->n > INT32_MAX || d->d <= 0 || d->ntrees <= 0 || d->nn <= 0 ||
       (d->dtype != DRPT_DTYPE_F32 && d->dtype != DRPT_DTYPE_U8) || !(d->tree_depth_ratio > 0) ||
-      (d->mode != DRPT_MODE_EXACT && d->mode != DRPT_MODE_FAST && d->mode != DRPT_MODE_MIXED)) {
+      (d->mode < DRPT_MODE_EXACT || d->mode > DRPT_MODE_FP32_LEAF)) {
     set_error("invalid descriptor (n=%lld d=%d ntrees=%d nn=%d dtype=%d mode=%d)",
               (long long)d->n, d->d, d->ntrees, d->nn, d->dtype, d->mode);
     return DRPT_ERR_INVALID_ARG;
@@ -315,6 +315,20 @@ drpt_status check_common(const drpt_build_desc *d) {
     set_error("nn = %d larger than %d", d->nn, kMaxK);
     return DRPT_ERR_UNSUPPORTED;
   }
+  return DRPT_OK;
+}
+
+// Global depth whose 2^(gd-1) leaves hold at most about `leaf_size` points
+// each (mixed and FP32-leaf modes).
+drpt_status leaf_depth(int64_t n, int leaf_size_in, int *gd_out) {
+  const int leaf_size = leaf_size_in > 0 ? leaf_size_in : 512;
+  int gd = 1;
+  while (gd < 30 && ((int64_t)1 << (gd - 1)) * leaf_size < n) ++gd;
+  if (gd > std::log2((double)n)) {
+    set_error("global depth %d outside [1, log2(%lld)]", gd, (long long)n);
+    return DRPT_ERR_DEPTH_OUT_OF_RANGE;
+  }
+  *gd_out = gd;
   return DRPT_OK;
 }
 
@@ -335,14 +349,8 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
     set_error("mixed mode supports d <= 256 (got %d)", d);
     return DRPT_ERR_UNSUPPORTED;
   }
-  const int leaf_size = desc->leaf_size > 0 ? desc->leaf_size : 512;
-  // leaves = 2^(gd-1) >= n / leaf_size
-  int gd = 1;
-  while (gd < 30 && ((int64_t)1 << (gd - 1)) * leaf_size < n) ++gd;
-  if (gd > std::log2((double)n)) {
-    set_error("mixed mode: global depth %d outside [1, log2(%lld)]", gd, (long long)n);
-    return DRPT_ERR_DEPTH_OUT_OF_RANGE;
-  }
+  int gd = 0;
+  DRPT_TRY(leaf_depth(n, desc->leaf_size, &gd));
   const int nleaf = 1 << (gd - 1);
   const int kp = nn <= 10 ? 16 : 32;  // running candidates per point, re-ranked at the end
   const int L = gd * T;
@@ -456,6 +464,73 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
   return DRPT_OK;
 }
 
+// FP32 whole-leaf pipeline (DRPT_MODE_FP32_LEAF): the mixed form's trees,
+// every global leaf brute-forced by the exact FP32 leaf kernel, cross-tree
+// merge.
+drpt_status run_fp32_leaf(drpt_ctx *c, const drpt_build_desc *desc, const void *X, int32_t *oi,
+                          float *od, drpt_stats *stats, cudaStream_t s) {
+  const int64_t n = desc->n;
+  const int d = desc->d, T = desc->ntrees, nn = desc->nn;
+  int gd = 0;
+  DRPT_TRY(leaf_depth(n, desc->leaf_size, &gd));
+  const int nleaf = 1 << (gd - 1);
+  const int L = gd * T;
+  const float density = (float)(desc->density == 0 ? 1.0 / std::sqrt((double)d) : desc->density);
+  cudaEvent_t *ev = c->ev;
+  const int launches0 = c->launches;
+  DRPT_CUDA(cudaEventRecord(ev[1], s));
+  std::vector<float> B((size_t)d * L);
+  host_projection_matrix(desc->seed, d, L, density, B.data());
+  std::vector<int32_t> cols;
+  for (int t = 0; t < T; ++t)
+    for (int l = 0; l + 1 < gd; ++l) cols.push_back(t * gd + l);
+  float *P = nullptr;
+  DRPT_TRY(ws_get(c, "P", std::max<size_t>(cols.size(), 1) * n, &P));
+  if (!cols.empty()) DRPT_TRY(project_cols(c, X, desc->dtype, n, d, B.data(), L, cols, P, s));
+  int32_t *order, *goff;
+  DRPT_TRY(global_trees(c, P, n, T, gd, 0, nullptr, &order, &goff, s));
+  DRPT_CUDA(cudaEventRecord(ev[2], s));
+  DRPT_CUDA(cudaEventRecord(ev[3], s));
+  int32_t *cidx;
+  float *cdist;
+  DRPT_TRY(ws_get(c, "cand_idx", (size_t)n * T * nn, &cidx));
+  DRPT_TRY(ws_get(c, "cand_dist", (size_t)n * T * nn, &cdist));
+  LeafKnnArgs ka{X, desc->dtype, n, d, T, nn, order, goff, nleaf, cidx, cdist};
+  DRPT_TRY(launch_leaf_knn_exact(ka, s));
+  c->launches += leaf_knn_exact_kernels();
+  DRPT_CUDA(cudaEventRecord(ev[4], s));
+  DRPT_TRY(launch_merge(cidx, cdist, n, T, nn, nn, oi, od, s));
+  c->launches += 1;
+  DRPT_CUDA(cudaEventRecord(ev[5], s));
+  DRPT_CUDA(cudaStreamSynchronize(s));
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->tree_depth = gd;
+    stats->global_depth = gd;
+    stats->n_global_leaves = nleaf;
+    stats->n_final_leaves = nleaf;
+    std::vector<int32_t> h((size_t)T * (nleaf + 1));
+    DRPT_CUDA(cudaMemcpy(h.data(), goff, h.size() * 4, cudaMemcpyDeviceToHost));
+    int64_t sq = 0, mn = INT64_MAX;
+    int mx = 0;
+    for (int t = 0; t < T; ++t)
+      for (int j = 0; j < nleaf; ++j) {
+        const int64_t m = h[(size_t)t * (nleaf + 1) + j + 1] - h[(size_t)t * (nleaf + 1) + j];
+        sq += m * m;
+        if (m > 0) mn = std::min(mn, m);
+        mx = std::max<int>(mx, (int)m);
+      }
+    stats->sum_leaf_sq = sq;
+    stats->min_global_leaf = mn;
+    stats->max_final_leaf = mx;
+    stats->kernels_launched = c->launches - launches0;
+    stats->ms_global = elapsed(ev[1], ev[2]);
+    stats->ms_leaf_knn = elapsed(ev[3], ev[4]);
+    stats->ms_merge = elapsed(ev[4], ev[5]);
+  }
+  return DRPT_OK;
+}
+
 }  // namespace
 }  // namespace drpt
 
@@ -518,8 +593,9 @@ drpt_status drpt_build_graph(drpt_ctx *c, const drpt_build_desc *desc, const voi
   const int64_t n = desc->n;
   const int d = desc->d, T = desc->ntrees, nn = desc->nn;
   const int exact = desc->mode == DRPT_MODE_EXACT;
-  Geometry g;
-  DRPT_TRY(geometry(n, desc->tree_depth, desc->tree_depth_ratio, &g));
+  Geometry g{};
+  if (desc->mode == DRPT_MODE_EXACT || desc->mode == DRPT_MODE_FAST)
+    DRPT_TRY(geometry(n, desc->tree_depth, desc->tree_depth_ratio, &g));
   const int L = g.gd * T;
   const float density = (float)(desc->density == 0 ? 1.0 / std::sqrt((double)d) : desc->density);
   const int launches0 = c->launches;
@@ -536,7 +612,7 @@ drpt_status drpt_build_graph(drpt_ctx *c, const drpt_build_desc *desc, const voi
     X = xd;
   }
 
-  if (desc->mode == DRPT_MODE_MIXED) {
+  if (desc->mode == DRPT_MODE_MIXED || desc->mode == DRPT_MODE_FP32_LEAF) {
     int32_t *oi = out_idx;
     float *od = out_dist;
     if (!desc->out_on_device) {
@@ -545,7 +621,8 @@ drpt_status drpt_build_graph(drpt_ctx *c, const drpt_build_desc *desc, const voi
     } else if (!od) {
       DRPT_TRY(ws_get(c, "out_dist", (size_t)n * nn, &od));
     }
-    DRPT_TRY(run_mixed(c, desc, X, oi, od, stats, s));
+    if (desc->mode == DRPT_MODE_MIXED) DRPT_TRY(run_mixed(c, desc, X, oi, od, stats, s));
+    else DRPT_TRY(run_fp32_leaf(c, desc, X, oi, od, stats, s));
     if (!desc->out_on_device) {
       DRPT_CUDA(cudaMemcpyAsync(out_idx, oi, (size_t)n * nn * 4, cudaMemcpyDeviceToHost, s));
       if (out_dist)

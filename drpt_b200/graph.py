@@ -83,7 +83,8 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
     if local_seeds is not None:
         seeds_arr = (ctypes.c_uint32 * ntrees)(*[int(s) & 0xFFFFFFFF for s in local_seeds])
         desc.local_seeds = seeds_arr
-    desc.mode = {"exact": _lib.MODE_EXACT, "fast": _lib.MODE_FAST, "mixed": _lib.MODE_MIXED}[mode]
+    desc.mode = {"exact": _lib.MODE_EXACT, "fast": _lib.MODE_FAST, "mixed": _lib.MODE_MIXED,
+                 "fp32_leaf": _lib.MODE_FP32_LEAF}[mode]
     desc.leaf_size = leaf_size
     desc.data_on_device = 1 if on_dev else 0
     desc.out_on_device = desc.data_on_device

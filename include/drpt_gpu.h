@@ -67,7 +67,12 @@ typedef enum {
    * or 32 candidates per tree and point; the merged 2*nn best are re-ranked
    * with exact FP32 distances and the k-th boundary is checked in FP64.  No
    * positional local split.  nn <= 16, d <= 256. */
-  DRPT_MODE_MIXED = 2
+  DRPT_MODE_MIXED = 2,
+  /* The mixed form's method in plain FP32: the same global trees and whole
+   * global leaves, brute-forced with the exact sequential FP32 distance of
+   * the plain form on the CUDA cores (no tensor cores, no re-rank).  The
+   * equal-recall FP32 counterpart of DRPT_MODE_MIXED. */
+  DRPT_MODE_FP32_LEAF = 3
 } drpt_mode;
 
 typedef struct drpt_ctx drpt_ctx;
@@ -89,7 +94,8 @@ typedef struct {
   int32_t data_on_device;     /* 1: `data` is device memory; 0: host memory */
   int32_t out_on_device;      /* 1: outputs are device memory; 0: host */
   void *stream;               /* cudaStream_t to run on; NULL = legacy default */
-  int32_t leaf_size;          /* mixed mode: target global leaf size (0 = 512) */
+  int32_t leaf_size;          /* mixed and FP32-leaf modes: target global leaf
+                                 size (0 = 512) */
   int32_t reserved;
 } drpt_build_desc;
 

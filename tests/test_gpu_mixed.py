@@ -87,3 +87,19 @@ def test_mixed_limits_are_reported(torch):
     with pytest.raises(DrptError) as e:
         build_graph(X, 2, 20, 1, mode="mixed")
     assert e.value.status == 8
+
+
+def test_mixed_matches_its_fp32_counterpart(torch, clustered):
+    """Same trees and leaves: the FP32 whole-leaf form returns the exact k
+    best of the candidate set; the mixed form (BF16 ranking, FP32 re-rank)
+    can only miss a few of them and never returns a closer list."""
+    X, Xd = clustered
+    im, dm, _ = build_graph(Xd, 4, 10, 21, mode="mixed", leaf_size=1024)
+    i3, d3, _ = build_graph(Xd, 4, 10, 21, mode="fp32_leaf", leaf_size=1024)
+    torch.cuda.synchronize()
+    im, dm, i3, d3 = (t.cpu().numpy() for t in (im, dm, i3, d3))
+    assert (d3 <= dm).all()                     # exact k best of the same candidates
+    same = np.mean([len(np.intersect1d(a, b)) / 10.0 for a, b in zip(im, i3)])
+    assert same >= 0.99, same
+    for p in (0, 5, 999):
+        assert d3[p, 0] == _exact_fp32(X[p], X[i3[p, 0]])
