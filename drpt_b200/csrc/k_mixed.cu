@@ -382,32 +382,48 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
       if (tree > 0) thr = run_dist[(int64_t)my_pt * KP + KP - 1] - nr;
     }
     const float thr0 = thr;
-    // Pending candidates: a passing candidate is stored at the row's next
-    // free slot by a predicated shared-memory store (no branch); slot
-    // addresses are 32-bit shared-window offsets.
+    // Pending candidates: a passing candidate is stored at the next free slot
+    // of one of two per-row lanes of the buffer (even and odd columns, so two
+    // independent append chains) by a predicated shared-memory store, no
+    // branch; slot addresses are 32-bit shared-window offsets.
+    constexpr int kHalf = kBufCap / 2;
     uint2 *const pbase = buf + row;
-    const uint32_t abase = smem_u32(pbase);
-    uint32_t aslot = abase;
-    auto pending = [&]() { return (int)((aslot - abase) / (kTM * 8)); };
+    const uint32_t abase0 = smem_u32(pbase), abase1 = abase0 + kHalf * kTM * 8;
+    uint32_t aslot0 = abase0, aslot1 = abase1;
+    auto pending0 = [&]() { return (int)((aslot0 - abase0) / (kTM * 8)); };
+    auto pending1 = [&]() { return (int)((aslot1 - abase1) / (kTM * 8)); };
     auto flush = [&]() {
-      const int cnt = pending();
-      const int mx = __reduce_max_sync(kFull, cnt);
-      for (int base = 0; base < mx; base += 16) {
+      const int c0 = pending0(), c1 = pending1();
+      const int mx = __reduce_max_sync(kFull, max(c0, c1));
+      for (int base = 0; base < mx; base += 8) {
+        // 8 slots of each half make one batch of 16
         float sd[16];
         int32_t si[16];
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
-          const int slot = base + e;
-          const bool have = slot < cnt;
-          const uint2 ent = have ? pbase[slot * kTM] : make_uint2(0x7f800000u, 0xffffffffu);
+          const int half = e >> 3, slot = base + (e & 7);
+          const bool have = slot < (half ? c1 : c0);
+          const uint2 ent = have ? pbase[(half * kHalf + slot) * kTM]
+                                 : make_uint2(0x7f800000u, 0xffffffffu);
           sd[e] = __uint_as_float(ent.x);
           si[e] = (int32_t)ent.y;
         }
         bitonic_sort<16>(sd, si);
         bitonic_merge_into<KP, 16>(td, ti, sd, si);
       }
-      aslot = abase;
+      aslot0 = abase0;
+      aslot1 = abase1;
       thr = fminf(thr0, td[KP - 1]);
+    };
+    auto append = [&](uint32_t &aslot, float sv, uint32_t pos) {
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "setp.lt.f32 p, %1, %2;\n\t"
+          "@p st.shared.v2.u32 [%0], {%3, %4};\n\t"
+          "@p add.u32 %0, %0, %5;\n\t}"
+          : "+r"(aslot)
+          : "f"(sv), "f"(thr), "r"(__float_as_uint(sv)), "r"(pos), "n"(kTM * 8)
+          : "memory");
     };
     // one 32-column chunk of scores; DIAG: the warp's diagonal chunk, where
     // lane l's own point is column l and is skipped
@@ -424,18 +440,11 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
             const int j = j4 + e;
             float sv = fmaf(-2.0f, v[j], ncs[e]);
             if (DIAG) sv = (j == lane) ? __int_as_float(0x7f800000) : sv;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\t"
-                "setp.lt.f32 p, %1, %2;\n\t"
-                "@p st.shared.v2.u32 [%0], {%3, %4};\n\t"
-                "@p add.u32 %0, %0, %5;\n\t}"
-                : "+r"(aslot)
-                : "f"(sv), "f"(thr), "r"(__float_as_uint(sv)), "r"((uint32_t)(cb + j)),
-                  "n"(kTM * 8)
-                : "memory");
+            if (j & 1) append(aslot1, sv, (uint32_t)(cb + j));
+            else append(aslot0, sv, (uint32_t)(cb + j));
           }
         }
-        if (__any_sync(kFull, pending() >= kBufCap - kCheck)) flush();
+        if (__any_sync(kFull, max(pending0(), pending1()) >= kHalf - kCheck / 2)) flush();
       }
     };
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
@@ -516,50 +525,60 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
 // exact FP32 distance of candidate j: the sequential sum, in dimension order,
 // of rounded squares of rounded differences, and its rounded square root.
 // d must be a multiple of 4.
-template <typename T, int D>
-__device__ __forceinline__ float exact_dist(const T *__restrict__ xp, const T *__restrict__ xc,
-                                            int d) {
-  // sequential FP32 sum over the dimensions in order (D > 0: compile-time d);
-  // rows are read four values at a time straight from global memory
-  float s = 0.0f;
-  const int dd = D > 0 ? D : d;
-#pragma unroll(D > 0 ? D / 4 : 4)
-  for (int i = 0; i < dd; i += 4) {
-    float a[4], b[4];
-    load4<T>(xp + i, a);
-    load4<T>(xc + i, b);
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const float df = __fsub_rn(b[e], a[e]);
-      s = __fadd_rn(s, __fmul_rn(df, df));
-    }
-  }
-  return __fsqrt_rn(s);
-}
-
-// G = 32 / K2 points per warp; lanes [g*K2, (g+1)*K2) serve point g, lane
-// j of a group computes candidate j from the two rows in global memory (the
-// query row is the same address for the whole group).  The K2 (distance,
-// index) pairs are then sorted with a bitonic network inside the group and
-// the first k kept; candidates whose FP32 distance lies within 2^-16 of the
-// k-th are re-ordered by an FP64 distance.  d must be a multiple of 4.
+// One warp per point.  For each candidate the warp reads the candidate row
+// with one coalesced pass (lane l holds dimensions 4l..4l+3 of every
+// 128-wide chunk), each lane adds its squared differences with fused
+// multiply-adds and a fixed butterfly adds the 32 lane sums: an FP32 distance
+// with pairwise summation, the same on every run.  Lane j then holds
+// candidate j (j < K2) and the K2 pairs are sorted with a bitonic network;
+// candidates whose distance lies within 2^-16 of the k-th are re-ordered by
+// an FP64 distance.  d must be a multiple of 4 and at most 256.
 template <typename T, int D, int K2>
 __global__ void __launch_bounds__(256) k_rerank(const T *__restrict__ X, int d,
                                                 const int32_t *__restrict__ visit, int64_t n,
                                                 const int32_t *__restrict__ ci, int k,
                                                 int32_t *__restrict__ oi, float *__restrict__ od) {
-  constexpr int G = 32 / K2;
   const int lane = threadIdx.x & 31;
-  const int g = lane / K2, j = lane % K2;
-  const int64_t wglob = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t w = wglob * G + g;       // this lane's point slot
-  if (wglob * G >= n) return;            // warp-uniform
-  const bool live = w < n;
-  const int32_t p = live ? (visit ? __ldg(visit + w) : (int32_t)w) : -1;
+  const int g = 0, j = lane;  // one point per warp: the group is the warp
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= n) return;  // warp-uniform
+  const bool live = true;
+  const int32_t p = visit ? __ldg(visit + w) : (int32_t)w;
   const float inf = __int_as_float(0x7f800000);
-  const int32_t c = live ? __ldg(ci + (int64_t)p * K2 + j) : -1;
+  const int32_t c = lane < K2 ? __ldg(ci + (int64_t)p * K2 + lane) : -1;
+  constexpr int NC = D > 0 ? (D + 127) / 128 : 2;  // 128-wide chunks (d <= 256)
+  float q[NC][4];
+  const T *xp = X + (int64_t)p * d;
+#pragma unroll
+  for (int h = 0; h < NC; ++h) {
+    const int c0 = h * 128 + 4 * lane;
+    q[h][0] = q[h][1] = q[h][2] = q[h][3] = 0.0f;
+    if (c0 < d) load4<T>(xp + c0, q[h]);
+  }
   float dist = inf;
-  if (c >= 0) dist = exact_dist<T, D>(X + (int64_t)p * d, X + (int64_t)c * d, d);
+#pragma unroll 4
+  for (int jj = 0; jj < K2; ++jj) {
+    const int32_t cj = __shfl_sync(kFull, c, jj);
+    if (cj < 0) continue;  // warp-uniform
+    const T *xc = X + (int64_t)cj * d;
+    float acc = 0.0f;
+#pragma unroll
+    for (int h = 0; h < NC; ++h) {
+      const int c0 = h * 128 + 4 * lane;
+      if (c0 < d) {
+        float v[4];
+        load4<T>(xc + c0, v);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float df = v[e] - q[h][e];
+          acc = fmaf(df, df, acc);
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+    if (lane == jj) dist = sqrtf(acc);
+  }
   int32_t id = c;
   // bitonic sort of K2 (dist, id) pairs inside the group, ascending
 #pragma unroll
@@ -632,8 +651,7 @@ template <typename T, int D, int K2>
 drpt_status launch_rerank_t(const void *X, int d, const int32_t *visit, int64_t n,
                             const int32_t *cand, int k, int32_t *out_idx, float *out_dist,
                             cudaStream_t s) {
-  constexpr int G = 32 / K2;
-  const int64_t warps = ceil_div(n, G);
+  const int64_t warps = n;
   const unsigned grid = (unsigned)ceil_div(warps * 32, 256);
   k_rerank<T, D, K2><<<grid, 256, 0, s>>>((const T *)X, d, visit, n, cand, k, out_idx, out_dist);
   DRPT_LAUNCH_CHECK();
@@ -646,7 +664,7 @@ drpt_status launch_rerank_d(const void *X, int d, const int32_t *visit, int64_t 
                             cudaStream_t s) {
   switch (d) {
     case 128: return launch_rerank_t<T, 128, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
-    case 96: return launch_rerank_t<T, 96, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
+    case 96: return launch_rerank_t<T, 128, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
     case 256: return launch_rerank_t<T, 256, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
     default: return launch_rerank_t<T, 0, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
   }
@@ -749,8 +767,8 @@ drpt_status launch_rerank(const void *X, int dtype, int d, const int32_t *visit,
     set_error("re-rank: %d candidates for k = %d unsupported (16 or 32)", K2, k);
     return DRPT_ERR_UNSUPPORTED;
   }
-  if (d % 4 != 0) {
-    set_error("re-rank needs d %% 4 == 0 (got %d)", d);
+  if (d % 4 != 0 || d > 256) {
+    set_error("re-rank needs d %% 4 == 0 and d <= 256 (got %d)", d);
     return DRPT_ERR_UNSUPPORTED;
   }
   if (dtype == DRPT_DTYPE_U8)

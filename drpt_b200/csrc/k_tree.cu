@@ -279,15 +279,24 @@ __global__ void __launch_bounds__(kThreads) k_stats_partial(TreeLevelArgs a) {
   }
 }
 
+// One warp per node: lanes take the node's units in turn, the lane partials
+// are then added in a fixed tree order.
 __global__ void k_bounds_fast(TreeLevelArgs a) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= (a.T << a.level)) return;
+  const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (g >= (a.T << a.level)) return;  // warp-uniform
   const NodeRange r = node_range(a, g);
   double s1 = 0.0, s2 = 0.0;
-  for (int u = a.node_ubase[g]; u < a.node_ubase[g + 1]; ++u) {
+  for (int u = a.node_ubase[g] + lane; u < a.node_ubase[g + 1]; u += 32) {
     s1 += a.unit_s[2 * u];
     s2 += a.unit_s[2 * u + 1];
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s1 += __shfl_xor_sync(kFull, s1, o);
+    s2 += __shfl_xor_sync(kFull, s2, o);
+  }
+  if (lane != 0) return;
   const double dn = (double)(r.hi - r.lo);
   double var = (s2 - s1 * (s1 / dn)) / (dn - 1.0);
   if (var < 0.0) var = 0.0;  // rounding can push a zero variance below 0 (NaN stays NaN)
@@ -327,16 +336,24 @@ __global__ void __launch_bounds__(kThreads) k_hist(TreeLevelArgs a) {
 }
 
 // ------------------------------------------------------------------ median
+// One warp per node: lanes add the counts of the node's units in turn
+// (integer counts, so the order is immaterial), lane 0 selects the median.
 __global__ void k_median(TreeLevelArgs a) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= (a.T << a.level)) return;
+  const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (g >= (a.T << a.level)) return;  // warp-uniform
   const NodeRange r = node_range(a, g);
   unsigned h[kBins];
 #pragma unroll
   for (int j = 0; j < kBins; ++j) h[j] = 0u;
-  for (int u = a.node_ubase[g]; u < a.node_ubase[g + 1]; ++u)
+  for (int u = a.node_ubase[g] + lane; u < a.node_ubase[g + 1]; u += 32)
 #pragma unroll
     for (int j = 0; j < kBins; ++j) h[j] += a.unit_hist[(int64_t)u * kBins + j];
+#pragma unroll
+  for (int j = 0; j < kBins; ++j)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) h[j] += __shfl_xor_sync(kFull, h[j], o);
+  if (lane != 0) return;
   float D[kBins];
 #pragma unroll
   for (int j = 0; j < kBins; ++j) D[j] = a.node_D[(int64_t)g * kBins + j];
@@ -374,21 +391,32 @@ __global__ void __launch_bounds__(kThreads) k_count(TreeLevelArgs a) {
 }
 
 // ------------------------------------------------------------------ node scan
+// One warp per node: exclusive prefix of the units' left counts in unit
+// order, 32 units per step with a running carry.
 __global__ void k_node_scan(TreeLevelArgs a) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= (a.T << a.level)) return;
+  const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (g >= (a.T << a.level)) return;  // warp-uniform
   const NodeRange r = node_range(a, g);
-  int acc = 0;
-  for (int u = a.node_ubase[g]; u < a.node_ubase[g + 1]; ++u) {
-    const int c = a.unit_left[u];
-    a.unit_lbase[u] = acc;
-    acc += c;
+  int carry = 0;
+  for (int u0 = a.node_ubase[g]; u0 < a.node_ubase[g + 1]; u0 += 32) {
+    const int u = u0 + lane;
+    const int c = u < a.node_ubase[g + 1] ? a.unit_left[u] : 0;
+    int x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, x, o);
+      if (lane >= o) x += y;
+    }
+    if (u < a.node_ubase[g + 1]) a.unit_lbase[u] = carry + x - c;
+    carry += __shfl_sync(kFull, x, 31);
   }
-  a.node_nleft[g] = acc;
+  if (lane != 0) return;
+  a.node_nleft[g] = carry;
   const int nodes = 1 << a.level, t = g >> a.level, s = g & (nodes - 1);
   int32_t *oo = a.off_out + (int64_t)t * (2 * nodes + 1);
   oo[2 * s] = (int32_t)r.lo;
-  oo[2 * s + 1] = (int32_t)(r.lo + acc);
+  oo[2 * s + 1] = (int32_t)(r.lo + carry);
   if (s == nodes - 1) oo[2 * nodes] = (int32_t)r.hi;
 }
 
@@ -469,18 +497,18 @@ drpt_status launch_tree_level(const TreeLevelArgs &a, int64_t max_units, cudaStr
     set_error("too many tree nodes at level %d", a.level);
     return DRPT_ERR_UNSUPPORTED;
   }
-  const unsigned U = (unsigned)max_units, gn = (unsigned)ceil_div(G, 128);
+  const unsigned U = (unsigned)max_units, gn = (unsigned)ceil_div(G * 32, 256);  // warp per node
   k_plan<<<1, 1024, 0, s>>>(a);
   if (a.exact) {
     k_stats_exact<<<(unsigned)G, kThreads, 0, s>>>(a);
   } else {
     k_stats_partial<<<U, kThreads, 0, s>>>(a);
-    k_bounds_fast<<<gn, 128, 0, s>>>(a);
+    k_bounds_fast<<<gn, 256, 0, s>>>(a);
   }
   k_hist<<<U, kThreads, 0, s>>>(a);
-  k_median<<<gn, 128, 0, s>>>(a);
+  k_median<<<gn, 256, 0, s>>>(a);
   k_count<<<U, kThreads, 0, s>>>(a);
-  k_node_scan<<<gn, 128, 0, s>>>(a);
+  k_node_scan<<<gn, 256, 0, s>>>(a);
   k_scatter<<<U, kThreads, 0, s>>>(a);
   DRPT_LAUNCH_CHECK();
   return DRPT_OK;
