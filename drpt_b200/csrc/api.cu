@@ -598,6 +598,13 @@ drpt_status drpt_build_graph(drpt_ctx *c, const drpt_build_desc *desc, const voi
     DRPT_TRY(geometry(n, desc->tree_depth, desc->tree_depth_ratio, &g));
   const int L = g.gd * T;
   const float density = (float)(desc->density == 0 ? 1.0 / std::sqrt((double)d) : desc->density);
+  // grow_local_trees takes the density as int (mdrpt.hpp:61-62): from 1 up the
+  // local matrices are not zero and the split is no longer positional.
+  if (exact && desc->density >= 1.0) {
+    set_error("density %g >= 1 makes the local projection matrices non-zero; exact mode "
+              "reproduces only the positional local split", desc->density);
+    return DRPT_ERR_LOCAL_MATRIX_NONZERO;
+  }
   const int launches0 = c->launches;
   cudaEvent_t *ev = c->ev;
   DRPT_CUDA(cudaEventRecord(ev[0], s));
