@@ -25,7 +25,7 @@ MODE_EXACT, MODE_FAST, MODE_MIXED, MODE_FP32_LEAF = 0, 1, 2, 3
 EXPORTS = [
     "drpt_version", "drpt_last_error", "drpt_ctx_create", "drpt_ctx_destroy", "drpt_build_graph",
     "drpt_host_projection", "drpt_project", "drpt_global_trees", "drpt_local_leaves",
-    "drpt_leaf_knn", "drpt_merge_candidates",
+    "drpt_leaf_knn", "drpt_merge_candidates", "drpt_global_trees_noalloc",
 ]
 
 
@@ -96,6 +96,7 @@ def load(path: str = LIB_PATH):
         L.drpt_local_leaves.argtypes = [vp, vp, vp, i64, i32, i32, i32, vp, vp, vp]
         L.drpt_leaf_knn.argtypes = [vp, vp, i32, i64, i32, i32, vp, vp, i32, i32, vp, vp, vp]
         L.drpt_merge_candidates.argtypes = [vp, vp, vp, i64, i32, i32, vp, vp, vp]
+        L.drpt_global_trees_noalloc.argtypes = [vp, i64, i32, i32, i32, vp, vp, vp, vp]
         for name in EXPORTS:
             fn = getattr(L, name)
             if name not in ("drpt_version", "drpt_last_error", "drpt_ctx_destroy"):

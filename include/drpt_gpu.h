@@ -179,6 +179,28 @@ drpt_status drpt_merge_candidates(drpt_ctx *ctx, const int32_t *cand_idx, const 
                                   int64_t n, int32_t T, int32_t k, int32_t *out_idx,
                                   float *out_dist, void *stream);
 
+/* drpt_global_trees without any device allocation.  No counterpart in the
+ * reference: it is for callers that cannot call cudaMalloc -- hosts whose
+ * own pool already holds the device's memory (a cudaMalloc would fail, or
+ * force the pool to give memory back and synchronise the device), and
+ * latency-bound loops that cannot take cudaMalloc's device-wide
+ * synchronisation.  Same arguments, meaning and outputs as
+ * drpt_global_trees (no context: it runs on the calling thread's current
+ * device, which must be the device of P, the outputs and `stream`).
+ *
+ * Scratch comes from a 64 MiB array that is part of the library's device
+ * image (every GPU that loads the library holds it until exit); `order` and
+ * `offsets` double as one side of the level ping-pong.  A build needs about
+ * 12*T*n bytes plus per-level tables; larger builds are rejected with
+ * DRPT_ERR_INVALID_ARG and a message naming the bytes needed (T*n up to
+ * about 5 million).  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  Every call shares the array: calls whose kernels overlap on the
+ * GPU (other streams, other host threads) race and must be serialised. */
+drpt_status drpt_global_trees_noalloc(const float *P, int64_t n, int32_t T, int32_t gd,
+                                      int32_t exact, int32_t *order, int32_t *offsets,
+                                      float *medians, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
