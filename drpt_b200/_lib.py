@@ -20,6 +20,7 @@ STATUS_NAMES = {
 }
 DTYPE_F32, DTYPE_U8 = 0, 1
 MODE_EXACT, MODE_FAST, MODE_MIXED, MODE_FP32_LEAF = 0, 1, 2, 3
+PRECISION_BF16, PRECISION_FP8_E4M3 = 0, 1
 
 # Every symbol include/drpt_gpu.h declares.
 EXPORTS = [
@@ -46,7 +47,7 @@ class BuildDesc(ctypes.Structure):
         ("density", ctypes.c_double), ("seed", ctypes.c_uint32),
         ("local_seeds", ctypes.POINTER(ctypes.c_uint32)), ("mode", ctypes.c_int32),
         ("data_on_device", ctypes.c_int32), ("out_on_device", ctypes.c_int32),
-        ("stream", ctypes.c_void_p), ("leaf_size", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("stream", ctypes.c_void_p), ("leaf_size", ctypes.c_int32), ("precision", ctypes.c_int32),
     ]
 
 

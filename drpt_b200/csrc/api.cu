@@ -321,6 +321,10 @@ drpt_status check_common(const drpt_build_desc *d) {
 // Global depth whose 2^(gd-1) leaves hold at most about `leaf_size` points
 // each (mixed and FP32-leaf modes).
 drpt_status leaf_depth(int64_t n, int leaf_size_in, int *gd_out) {
+  if (leaf_size_in < 0) {
+    set_error("leaf_size %d < 0", leaf_size_in);
+    return DRPT_ERR_INVALID_ARG;
+  }
   const int leaf_size = leaf_size_in > 0 ? leaf_size_in : 512;
   int gd = 1;
   while (gd < 30 && ((int64_t)1 << (gd - 1)) * leaf_size < n) ++gd;
@@ -340,15 +344,20 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
                       float *od, drpt_stats *stats, cudaStream_t s) {
   const int64_t n = desc->n;
   const int d = desc->d, T = desc->ntrees, nn = desc->nn;
-  if (nn > 16) {
-    set_error("mixed mode supports nn <= 16 (got %d)", nn);
+  if (nn > 32) {
+    set_error("mixed mode supports nn <= 32 (got %d)", nn);
     return DRPT_ERR_UNSUPPORTED;
   }
-  const int d_pad = (d + 63) / 64 * 64;
-  if (d_pad > 256) {
-    set_error("mixed mode supports d <= 256 (got %d)", d);
+  if (desc->precision != DRPT_PRECISION_BF16 && desc->precision != DRPT_PRECISION_FP8_E4M3) {
+    set_error("unknown precision %d", desc->precision);
+    return DRPT_ERR_INVALID_ARG;
+  }
+  const int fp8 = desc->precision == DRPT_PRECISION_FP8_E4M3;
+  if (d % 4 != 0 || d > 1024) {
+    set_error("mixed mode supports d %% 4 == 0 and d <= 1024 (got %d)", d);
     return DRPT_ERR_UNSUPPORTED;
   }
+  const int d_pad = mixed_d_pad(d, fp8);
   int gd = 0;
   DRPT_TRY(leaf_depth(n, desc->leaf_size, &gd));
   const int nleaf = 1 << (gd - 1);
@@ -380,8 +389,12 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
   a.nleaf = nleaf;
   a.T = T;
   a.kp = kp;
-  DRPT_TRY(ws_get(c, "mx_xb", (size_t)n * d_pad, &a.Xb));
+  a.fp8 = fp8;
+  uint8_t *xb = nullptr;
+  DRPT_TRY(ws_get(c, "mx_xb", (size_t)n * d_pad * (fp8 ? 1 : 2), &xb));
+  a.Xb = xb;
   DRPT_TRY(ws_get(c, "mx_nrm", (size_t)n, &a.nrm));
+  DRPT_TRY(ws_get(c, "mx_scl", fp8 ? (size_t)n : 1, &a.scl));
   const size_t tiles = (size_t)ceil_div(n, 128) + nleaf;
   DRPT_TRY(ws_get(c, "mx_tile_leaf", tiles, &a.tile_leaf));
   DRPT_TRY(ws_get(c, "mx_tile_r0", tiles, &a.tile_r0));

@@ -27,6 +27,7 @@
 // to the squared distances that are ranked (values of a few tens instead of a
 // few hundreds for the synthetic workloads).
 #include <cuda.h>
+#include <cuda_fp8.h>
 
 #include <algorithm>
 #include <type_traits>
@@ -66,29 +67,43 @@ __device__ __forceinline__ void load4<uint8_t>(const uint8_t *p, float *v) {
   v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
 }
 
-// One block per global leaf.  Warps take rows in turn; lane l owns the four
-// dimensions 4l..4l+3 of every 128-wide chunk (d <= 256, d % 4 == 0).  The
-// centre is the mean of the leaf's first (up to) kCentreRows rows -- it only
-// has to bring the values near zero -- summed per warp, the eight warp
-// partials added in warp order, so the result does not depend on scheduling.
-template <typename T>
+// Grid (leaves, splits): block (j, y) handles the y-th of gridDim.y row ranges
+// of global leaf j (several blocks per leaf when leaves are few).  Warps take
+// rows in turn; lane l owns the four
+// dimensions 4l..4l+3 of every 128-wide chunk (NCH chunks, d <= 128 * NCH,
+// d % 4 == 0).  The centre is the mean of the leaf's first (up to)
+// kCentreRows rows -- it only has to bring the values near zero -- summed per
+// warp, the eight warp partials added in warp order, so the result does not
+// depend on scheduling.
+//
+// BF16 output: the centred row rounded to BF16 (d_pad elements, zero-padded).
+// E4M3 output (FP8): the centred row divided by its scale
+// s = max|x - c| / 448 (448 = largest finite E4M3 value) and rounded to E4M3
+// with saturation (d_pad bytes, zero-padded); the scale goes to `scl`.  In
+// both cases `nrm` receives the squared norm of the row the tensor cores see
+// (dequantised for FP8), so that ||y||^2 - 2 x.y ranks the same values.
+template <typename T, int NCH, bool FP8>
 __global__ void __launch_bounds__(256) k_leaf_center(const T *__restrict__ X, int d, int d_pad,
                                                      const int32_t *__restrict__ order,
                                                      const int32_t *__restrict__ goff,
-                                                     __nv_bfloat16 *__restrict__ Xb,
-                                                     float *__restrict__ nrm) {
-  __shared__ float part[8][256];
-  __shared__ float mu[256];
+                                                     void *__restrict__ Xq,
+                                                     float *__restrict__ nrm,
+                                                     float *__restrict__ scl) {
+  constexpr int W = NCH * 128;
+  __shared__ float part[8][W];
+  __shared__ float mu[W];
   const int j = blockIdx.x;
   const int32_t lo = goff[j], hi = goff[j + 1];
   const int m = hi - lo;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+  float acc[NCH][4];
+#pragma unroll
+  for (int h = 0; h < NCH; ++h) acc[h][0] = acc[h][1] = acc[h][2] = acc[h][3] = 0.0f;
   const int mc = min(m, kCentreRows);
   for (int r = warp; r < mc; r += 8) {
     const T *src = X + (int64_t)__ldg(order + lo + r) * d;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < NCH; ++h) {
       const int c0 = h * 128 + 4 * lane;
       if (c0 < d) {
         float v[4];
@@ -99,25 +114,27 @@ __global__ void __launch_bounds__(256) k_leaf_center(const T *__restrict__ X, in
     }
   }
 #pragma unroll
-  for (int h = 0; h < 2; ++h)
+  for (int h = 0; h < NCH; ++h)
 #pragma unroll
     for (int e = 0; e < 4; ++e) part[warp][h * 128 + 4 * lane + e] = acc[h][e];
   __syncthreads();
-  if (threadIdx.x < 256) {
+  for (int i = threadIdx.x; i < W; i += 256) {
     float s = 0.0f;
-    for (int w = 0; w < 8; ++w) s += part[w][threadIdx.x];
-    mu[threadIdx.x] = mc > 0 ? s / (float)mc : 0.0f;
+    for (int w = 0; w < 8; ++w) s += part[w][i];
+    mu[i] = mc > 0 ? s / (float)mc : 0.0f;
   }
   __syncthreads();
-  constexpr int RB = 4;  // rows per warp step, loaded together
-  for (int r0w = warp * RB; r0w < m; r0w += 8 * RB) {
-    float v[RB][2][4];
+  constexpr int RB = NCH <= 2 ? 4 : 1;  // rows per warp step, loaded together
+  const int rb = (int)((int64_t)m * blockIdx.y / gridDim.y);
+  const int re = (int)((int64_t)m * (blockIdx.y + 1) / gridDim.y);
+  for (int r0w = rb + warp * RB; r0w < re; r0w += 8 * RB) {
+    float v[RB][NCH][4];
 #pragma unroll
     for (int q = 0; q < RB; ++q) {
       const int r = r0w + q;
-      const T *src = r < m ? X + (int64_t)__ldg(order + lo + r) * d : nullptr;
+      const T *src = r < re ? X + (int64_t)__ldg(order + lo + r) * d : nullptr;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      for (int h = 0; h < NCH; ++h) {
         const int c0 = h * 128 + 4 * lane;
         v[q][h][0] = v[q][h][1] = v[q][h][2] = v[q][h][3] = 0.0f;
         if (src && c0 < d) load4<T>(src + c0, v[q][h]);
@@ -126,25 +143,71 @@ __global__ void __launch_bounds__(256) k_leaf_center(const T *__restrict__ X, in
 #pragma unroll
     for (int q = 0; q < RB; ++q) {
       const int r = r0w + q;
-      float sq = 0.0f;
-      __nv_bfloat16 *dst = Xb + (int64_t)(lo + (r < m ? r : 0)) * d_pad;
+      const int64_t row = lo + (r < re ? r : 0);
+      float c[NCH][4];
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int c0 = h * 128 + 4 * lane;
-        if (c0 < d_pad) {
-          __nv_bfloat16 b[4];
+      for (int h = 0; h < NCH; ++h)
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            b[e] = __float2bfloat16_rn(c0 + e < d ? v[q][h][e] - mu[c0 + e] : 0.0f);
-            const float vr = __bfloat162float(b[e]);
-            sq = fmaf(vr, vr, sq);
-          }
-          if (r < m) *reinterpret_cast<uint2 *>(dst + c0) = *reinterpret_cast<const uint2 *>(b);
+        for (int e = 0; e < 4; ++e) {
+          const int col = h * 128 + 4 * lane + e;
+          c[h][e] = col < d ? v[q][h][e] - mu[col] : 0.0f;
         }
-      }
+      float sq = 0.0f;
+      if constexpr (FP8) {
+        float amax = 0.0f;
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(kFull, sq, o);
-      if (lane == 0 && r < m) nrm[lo + r] = sq;
+        for (int h = 0; h < NCH; ++h)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) amax = fmaxf(amax, fabsf(c[h][e]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(kFull, amax, o));
+        const float sc = amax > 0.0f ? amax / 448.0f : 1.0f;
+        const float inv = amax > 0.0f ? 448.0f / amax : 1.0f;
+        uint8_t *dst = static_cast<uint8_t *>(Xq) + row * d_pad;
+#pragma unroll
+        for (int h = 0; h < NCH; ++h) {
+          const int c0 = h * 128 + 4 * lane;
+          if (c0 < d_pad) {
+            const __nv_fp8x2_storage_t lo2 = __nv_cvt_float2_to_fp8x2(
+                make_float2(c[h][0] * inv, c[h][1] * inv), __NV_SATFINITE, __NV_E4M3);
+            const __nv_fp8x2_storage_t hi2 = __nv_cvt_float2_to_fp8x2(
+                make_float2(c[h][2] * inv, c[h][3] * inv), __NV_SATFINITE, __NV_E4M3);
+            const float2 a = __half22float2(__nv_cvt_fp8x2_to_halfraw2(lo2, __NV_E4M3));
+            const float2 b = __half22float2(__nv_cvt_fp8x2_to_halfraw2(hi2, __NV_E4M3));
+            sq = fmaf(a.x, a.x, sq);
+            sq = fmaf(a.y, a.y, sq);
+            sq = fmaf(b.x, b.x, sq);
+            sq = fmaf(b.y, b.y, sq);
+            if (r < re)
+              *reinterpret_cast<uint32_t *>(dst + c0) = (uint32_t)lo2 | ((uint32_t)hi2 << 16);
+          }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(kFull, sq, o);
+        if (lane == 0 && r < re) {
+          nrm[lo + r] = sq * sc * sc;
+          scl[lo + r] = sc;
+        }
+      } else {
+        __nv_bfloat16 *dst = static_cast<__nv_bfloat16 *>(Xq) + row * d_pad;
+#pragma unroll
+        for (int h = 0; h < NCH; ++h) {
+          const int c0 = h * 128 + 4 * lane;
+          if (c0 < d_pad) {
+            __nv_bfloat16 b[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              b[e] = __float2bfloat16_rn(c[h][e]);
+              const float vr = __bfloat162float(b[e]);
+              sq = fmaf(vr, vr, sq);
+            }
+            if (r < re) *reinterpret_cast<uint2 *>(dst + c0) = *reinterpret_cast<const uint2 *>(b);
+          }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(kFull, sq, o);
+        if (lane == 0 && r < re) nrm[lo + r] = sq;
+      }
     }
   }
 }
@@ -244,44 +307,68 @@ __device__ __forceinline__ void bitonic_merge_into(float *L, int32_t *Li, const 
     }
 }
 
+// Shared-memory layout.  Every operand tile is rows of 128 bytes (64 BF16 or
+// 128 E4M3 values of one 128-byte K block), 128-byte swizzled, 1024-byte
+// aligned.
+//   resident A (kb <= 4): A = kb K blocks of the 128 rows, loaded once per row
+//     tile; kStages stages of the kb K blocks of a 64-column B tile;
+//   streamed A (larger kb): kSStages stages, each one K block of A (16 KB)
+//     and of B (8 KB), so A is re-read from L2 for every column tile.
+constexpr int kSStages = 3;
+constexpr uint32_t kStreamA = kTM * 128, kStreamStage = kTM * 128 + kTN * 128;
+
 struct MmaSmem {
-  uint32_t a_off, b_off, buf_off, nrm_off, bar_off, total;
+  uint32_t a_off, b_off, buf_off, nrm_off, scl_off, bar_off, total;
 };
 
-__host__ __device__ inline MmaSmem mma_smem_layout(int kb) {
+__host__ __device__ inline MmaSmem mma_smem_layout(int kb, bool stream) {
   MmaSmem L;
   L.a_off = 0;
-  L.b_off = L.a_off + (uint32_t)kb * kTM * 128;
-  L.buf_off = L.b_off + (uint32_t)kStages * kb * kTN * 128;
+  if (stream) {
+    L.b_off = kStreamA;  // inside each stage
+    L.buf_off = kSStages * kStreamStage;
+  } else {
+    L.b_off = L.a_off + (uint32_t)kb * kTM * 128;
+    L.buf_off = L.b_off + (uint32_t)kStages * kb * kTN * 128;
+  }
   L.nrm_off = L.buf_off + kTM * kBufCap * 8;
-  L.bar_off = L.nrm_off + kEpiWarps * kTN * 4;
+  L.scl_off = L.nrm_off + kEpiWarps * kTN * 4;
+  L.bar_off = L.scl_off + kEpiWarps * kTN * 4;
   L.total = L.bar_off + 16 * 8 + 16;
   return L;
 }
 
-template <int KP>
+// KP: candidates kept per row and tree.  STREAM: streamed A.  FP8: E4M3
+// operands with per-row scales `scl` (scores are then scaled by the row's and
+// the column's scale); otherwise BF16.
+template <int KP, bool STREAM, bool FP8>
 __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
     const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
     const int32_t *__restrict__ goff, const int32_t *__restrict__ order,
-    const float *__restrict__ nrm, const int32_t *__restrict__ tile_leaf,
-    const int32_t *__restrict__ tile_r0, const int32_t *__restrict__ n_tiles, int kb, int tree,
-    int32_t *__restrict__ run_idx, float *__restrict__ run_dist, int *err) {
+    const float *__restrict__ nrm, const float *__restrict__ scl,
+    const int32_t *__restrict__ tile_leaf, const int32_t *__restrict__ tile_r0,
+    const int32_t *__restrict__ n_tiles, int kb, int tree, int32_t *__restrict__ run_idx,
+    float *__restrict__ run_dist, int *err) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
-  const MmaSmem L = mma_smem_layout(kb);
+  const MmaSmem L = mma_smem_layout(kb, STREAM);
   uint8_t *sA = smem + L.a_off;
   uint8_t *sB = smem + L.b_off;
   uint2 *buf = reinterpret_cast<uint2 *>(smem + L.buf_off);  // [slot][row]: (value bits, position)
   float *nbuf = reinterpret_cast<float *>(smem + L.nrm_off);  // [warp][kTN] column norms of a tile
+  float *sbuf = reinterpret_cast<float *>(smem + L.scl_off);  // [warp][kTN] column scales (FP8)
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L.bar_off);
+  constexpr int kMaxStages = kStages > kSStages ? kStages : kSStages;
   uint64_t *full_a = bars + 0;
-  uint64_t *full_b = bars + 1;             // kStages
-  uint64_t *empty_b = bars + 1 + kStages;  // kStages
-  uint64_t *acc_full = bars + 1 + 2 * kStages;
+  uint64_t *full_b = bars + 1;                // kMaxStages
+  uint64_t *empty_b = bars + 1 + kMaxStages;  // kMaxStages
+  uint64_t *acc_full = bars + 1 + 2 * kMaxStages;
   uint64_t *acc_empty = acc_full + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 16);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 16) + 1;
+  constexpr int NS = STREAM ? kSStages : kStages;
+  constexpr int kKE = FP8 ? 128 : 64;  // elements per 128-byte K block
 
   const int u = blockIdx.x;
   if (u >= *n_tiles) return;  // uniform for the whole block
@@ -293,7 +380,7 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
 
   if (threadIdx.x == 0) {
     mbar_init(full_a, 1);
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < NS; ++s) {
       mbar_init(full_b + s, 1);
       mbar_init(empty_b + s, 1);
     }
@@ -317,40 +404,83 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
   if (warp == kEpiWarps) {
     // ---- TMA producer
     if (lane == 0) {
-      mbar_arrive_expect_tx(full_a, a_bytes);
-      for (int q = 0; q < kb; ++q) tma_load_2d(sA + q * kTM * 128, &tmA, full_a, q * 64, lo + r0);
-      for (int c = 0; c < nct && !*abort_flag; ++c) {
-        const int s = c % kStages;
-        if (c >= kStages && !mbar_wait(empty_b + s, ((c / kStages) - 1) & 1)) {
-          *abort_flag = 1;
-          break;
+      if constexpr (STREAM) {
+        // stage i = (column tile c, K block q) with i = c * kb + q
+        const int total = nct * kb;
+        for (int i = 0; i < total && !*abort_flag; ++i) {
+          const int s = i % NS, c = i / kb, q = i - c * kb;
+          if (i >= NS && !mbar_wait(empty_b + s, ((i / NS) - 1) & 1)) {
+            *abort_flag = 1;
+            break;
+          }
+          uint8_t *st = smem + (size_t)s * kStreamStage;
+          mbar_arrive_expect_tx(full_b + s, kStreamStage);
+          tma_load_2d(st, &tmA, full_b + s, q * kKE, lo + r0);
+          tma_load_2d(st + kStreamA, &tmB, full_b + s, q * kKE, lo + c * kTN);
         }
-        uint8_t *dst = sB + s * b_bytes;
-        mbar_arrive_expect_tx(full_b + s, b_bytes);
+      } else {
+        mbar_arrive_expect_tx(full_a, a_bytes);
         for (int q = 0; q < kb; ++q)
-          tma_load_2d(dst + q * kTN * 128, &tmB, full_b + s, q * 64, lo + c * kTN);
+          tma_load_2d(sA + q * kTM * 128, &tmA, full_a, q * kKE, lo + r0);
+        for (int c = 0; c < nct && !*abort_flag; ++c) {
+          const int s = c % NS;
+          if (c >= NS && !mbar_wait(empty_b + s, ((c / NS) - 1) & 1)) {
+            *abort_flag = 1;
+            break;
+          }
+          uint8_t *dst = sB + s * b_bytes;
+          mbar_arrive_expect_tx(full_b + s, b_bytes);
+          for (int q = 0; q < kb; ++q)
+            tma_load_2d(dst + q * kTN * 128, &tmB, full_b + s, q * kKE, lo + c * kTN);
+        }
       }
     }
   } else if (warp == kEpiWarps + 1) {
-    // ---- MMA issuer
+    // ---- MMA issuer: 4 instructions per 128-byte K block (K = 16 BF16 or
+    // 32 E4M3 values, 32 bytes each)
     if (lane == 0) {
-      constexpr uint32_t idesc = idesc_bf16_f32(kTM, kTN);
-      const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
-      bool ok = mbar_wait(full_a, 0);
-      for (int c = 0; ok && c < nct && !*abort_flag; ++c) {
-        const int s = c % kStages, b = c & 1;
-        ok = mbar_wait(full_b + s, (c / kStages) & 1);
-        if (ok && c >= 2) ok = mbar_wait(acc_empty + b, ((c >> 1) - 1) & 1);
-        if (!ok) break;
-        tc_fence_after();
-        const uint32_t bs = b_base + s * b_bytes;
-        for (int q = 0; q < kb; ++q)
+      constexpr uint32_t idesc = FP8 ? idesc_e4m3_f32(kTM, kTN) : idesc_bf16_f32(kTM, kTN);
+      auto mma = [&](uint32_t d, uint64_t ad, uint64_t bd, uint32_t acc) {
+        if constexpr (FP8) mma_e4m3(d, ad, bd, idesc, acc);
+        else mma_bf16(d, ad, bd, idesc, acc);
+      };
+      bool ok = true;
+      if constexpr (STREAM) {
+        for (int c = 0; ok && c < nct && !*abort_flag; ++c) {
+          const int b = c & 1;
+          if (c >= 2) ok = mbar_wait(acc_empty + b, ((c >> 1) - 1) & 1);
+          for (int q = 0; ok && q < kb; ++q) {
+            const int i = c * kb + q, s = i % NS;
+            ok = mbar_wait(full_b + s, (i / NS) & 1);
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t as = smem_u32(smem + (size_t)s * kStreamStage), bs = as + kStreamA;
 #pragma unroll
-          for (int k = 0; k < 4; ++k)
-            mma_bf16(tmem + b * kTN, desc_k_sw128(a_base + q * kTM * 128 + k * 32),
-                     desc_k_sw128(bs + q * kTN * 128 + k * 32), idesc, (q | k) ? 1u : 0u);
-        mma_commit(empty_b + s);
-        mma_commit(acc_full + b);
+            for (int k = 0; k < 4; ++k)
+              mma(tmem + b * kTN, desc_k_sw128(as + k * 32), desc_k_sw128(bs + k * 32),
+                  (q | k) ? 1u : 0u);
+            mma_commit(empty_b + s);
+          }
+          if (ok) mma_commit(acc_full + b);
+        }
+      } else {
+        const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
+        ok = mbar_wait(full_a, 0);
+        for (int c = 0; ok && c < nct && !*abort_flag; ++c) {
+          const int s = c % NS, b = c & 1;
+          ok = mbar_wait(full_b + s, (c / NS) & 1);
+          if (ok && c >= 2) ok = mbar_wait(acc_empty + b, ((c >> 1) - 1) & 1);
+          if (!ok) break;
+          tc_fence_after();
+          const uint32_t bs = b_base + s * b_bytes;
+          for (int q = 0; q < kb; ++q)
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+              mma(tmem + b * kTN, desc_k_sw128(a_base + q * kTM * 128 + k * 32),
+                  desc_k_sw128(bs + q * kTN * 128 + k * 32), (q | k) ? 1u : 0u);
+          mma_commit(empty_b + s);
+          mma_commit(acc_full + b);
+        }
       }
       if (!ok) *abort_flag = 1;
     }
@@ -374,11 +504,12 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
     // (rows past the leaf get -inf and keep nothing)
     float thr = rvalid ? __int_as_float(0x7f800000) : -__int_as_float(0x7f800000);
     int32_t my_pos = -1, my_pt = -1;
-    float nr = 0.0f;
+    float nr = 0.0f, m2s = -2.0f;  // FP8: -2 x the row's scale
     if (rvalid) {
       my_pos = lo + r0 + row;
       my_pt = __ldg(order + my_pos);
       nr = __ldg(nrm + my_pos);
+      if constexpr (FP8) m2s = -2.0f * __ldg(scl + my_pos);
       if (tree > 0) thr = run_dist[(int64_t)my_pt * KP + KP - 1] - nr;
     }
     const float thr0 = thr;
@@ -427,18 +558,24 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
     };
     // one 32-column chunk of scores; DIAG: the warp's diagonal chunk, where
     // lane l's own point is column l and is skipped
-    auto scan = [&](const float *v, const float *wn, int cb, auto diag_tag) {
+    auto scan = [&](const float *v, const float *wn, const float *ws, int cb, auto diag_tag) {
       constexpr bool DIAG = decltype(diag_tag)::value;
 #pragma unroll
       for (int h = 0; h < 32; h += kCheck) {
 #pragma unroll
         for (int j4 = h; j4 < h + kCheck; j4 += 4) {
           const float4 nc4 = *reinterpret_cast<const float4 *>(wn + j4);
+          float4 sc4 = make_float4(0.f, 0.f, 0.f, 0.f);
+          if constexpr (FP8) sc4 = *reinterpret_cast<const float4 *>(ws + j4);
+          const float scs[4] = {sc4.x, sc4.y, sc4.z, sc4.w};
+          (void)scs;
           const float ncs[4] = {nc4.x, nc4.y, nc4.z, nc4.w};
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             const int j = j4 + e;
-            float sv = fmaf(-2.0f, v[j], ncs[e]);
+            float sv;
+            if constexpr (FP8) sv = fmaf(m2s * scs[e], v[j], ncs[e]);
+            else sv = fmaf(-2.0f, v[j], ncs[e]);
             if (DIAG) sv = (j == lane) ? __int_as_float(0x7f800000) : sv;
             if (j & 1) append(aslot1, sv, (uint32_t)(cb + j));
             else append(aslot0, sv, (uint32_t)(cb + j));
@@ -458,11 +595,13 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
       // this tile's column norms, staged per warp (16-byte aligned reads);
       // columns past the leaf carry an infinite norm and so never pass
       float *wn = nbuf + warp * kTN;
+      float *ws = sbuf + warp * kTN;
       __syncwarp();
 #pragma unroll
       for (int h = 0; h < kTN; h += 32) {
         const int col = c * kTN + h + lane;
         wn[h + lane] = col < m ? __ldg(nrm + lo + col) : __int_as_float(0x7f800000);
+        if constexpr (FP8) ws[h + lane] = col < m ? __ldg(scl + lo + col) : 0.0f;
       }
       __syncwarp();
 #pragma unroll
@@ -472,9 +611,9 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
         const int cb = c * kTN + q * 32;
         // the warp's 32 rows sit in one 32-column chunk of the diagonal
         if (cb == r0 + warp * 32)
-          scan(v, wn + q * 32, lo + cb, std::true_type{});
+          scan(v, wn + q * 32, ws + q * 32, lo + cb, std::true_type{});
         else
-          scan(v, wn + q * 32, lo + cb, std::false_type{});
+          scan(v, wn + q * 32, ws + q * 32, lo + cb, std::false_type{});
       }
       tc_fence_before();
       mbar_arrive(acc_empty + b);
@@ -546,7 +685,7 @@ __global__ void __launch_bounds__(256) k_rerank(const T *__restrict__ X, int d,
   const int32_t p = visit ? __ldg(visit + w) : (int32_t)w;
   const float inf = __int_as_float(0x7f800000);
   const int32_t c = lane < K2 ? __ldg(ci + (int64_t)p * K2 + lane) : -1;
-  constexpr int NC = D > 0 ? (D + 127) / 128 : 2;  // 128-wide chunks (d <= 256)
+  constexpr int NC = (D + 127) / 128;  // 128-wide chunks (d <= D <= 1024)
   float q[NC][4];
   const T *xp = X + (int64_t)p * d;
 #pragma unroll
@@ -662,12 +801,11 @@ template <typename T, int K2>
 drpt_status launch_rerank_d(const void *X, int d, const int32_t *visit, int64_t n,
                             const int32_t *cand, int k, int32_t *out_idx, float *out_dist,
                             cudaStream_t s) {
-  switch (d) {
-    case 128: return launch_rerank_t<T, 128, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
-    case 96: return launch_rerank_t<T, 128, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
-    case 256: return launch_rerank_t<T, 256, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
-    default: return launch_rerank_t<T, 0, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
-  }
+  // D: an upper bound of d in whole 128-value chunks (the kernel guards c0 < d)
+  if (d <= 128) return launch_rerank_t<T, 128, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
+  if (d <= 256) return launch_rerank_t<T, 256, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
+  if (d <= 512) return launch_rerank_t<T, 512, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
+  return launch_rerank_t<T, 1024, K2>(X, d, visit, n, cand, k, out_idx, out_dist, s);
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
@@ -688,18 +826,21 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-drpt_status make_tmap(CUtensorMap *map, const void *base, int64_t rows, int d_pad, int box_rows) {
+drpt_status make_tmap(CUtensorMap *map, const void *base, int64_t rows, int d_pad, int box_rows,
+                      bool fp8) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) {
     set_error("cuTensorMapEncodeTiled is not available");
     return DRPT_ERR_CUDA;
   }
+  const int esz = fp8 ? 1 : 2;
   cuuint64_t dims[2] = {(cuuint64_t)d_pad, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)d_pad * 2};
-  cuuint32_t box[2] = {64, (cuuint32_t)box_rows};
+  cuuint64_t strides[1] = {(cuuint64_t)d_pad * esz};
+  cuuint32_t box[2] = {(cuuint32_t)(128 / esz), (cuuint32_t)box_rows};  // 128-byte rows
   cuuint32_t estr[2] = {1, 1};
-  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides,
-                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+  CUresult r = fn(map, fp8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                  const_cast<void *>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -708,56 +849,89 @@ drpt_status make_tmap(CUtensorMap *map, const void *base, int64_t rows, int d_pa
   return DRPT_OK;
 }
 
-}  // namespace
+template <typename T, int NCH>
+void center_t(const MixedTreeArgs &a, cudaStream_t s) {
+  // enough blocks for about four per SM, at least 64 rows per block
+  const int64_t mean = a.n / a.nleaf;
+  const int64_t split = std::max<int64_t>(
+      1, std::min<int64_t>(ceil_div(4 * 148, a.nleaf), mean / 64));
+  const dim3 grid((unsigned)a.nleaf, (unsigned)split);
+  if (a.fp8)
+    k_leaf_center<T, NCH, true><<<grid, 256, 0, s>>>((const T *)a.X, a.d, a.d_pad, a.order,
+                                                     a.goff, a.Xb, a.nrm, a.scl);
+  else
+    k_leaf_center<T, NCH, false><<<grid, 256, 0, s>>>((const T *)a.X, a.d, a.d_pad, a.order,
+                                                      a.goff, a.Xb, a.nrm, a.scl);
+}
 
-drpt_status launch_leaf_center(const MixedTreeArgs &a, cudaStream_t s) {
-  if (a.d % 4 != 0 || a.d > 256) {
-    set_error("mixed mode needs d %% 4 == 0 and d <= 256 (got %d)", a.d);
+template <typename T>
+void center_d(const MixedTreeArgs &a, cudaStream_t s) {
+  if (a.d_pad <= 256) center_t<T, 2>(a, s);
+  else if (a.d_pad <= 512) center_t<T, 4>(a, s);
+  else center_t<T, 8>(a, s);
+}
+
+template <int KP, bool STREAM, bool FP8>
+drpt_status mma_t(const MixedTreeArgs &a, const CUtensorMap &tmA, const CUtensorMap &tmB, int kb,
+                  cudaStream_t s) {
+  const MmaSmem L = mma_smem_layout(kb, STREAM);
+  const size_t smem = L.total + 1024;
+  if (smem > 227 * 1024) {
+    set_error("mixed leaf kernel: %zu bytes of shared memory needed", smem);
     return DRPT_ERR_UNSUPPORTED;
   }
-  const size_t smem = 0;
-  if (a.dtype == DRPT_DTYPE_U8)
-    k_leaf_center<uint8_t><<<a.nleaf, 256, smem, s>>>((const uint8_t *)a.X, a.d, a.d_pad, a.order,
-                                                       a.goff, a.Xb, a.nrm);
-  else
-    k_leaf_center<float><<<a.nleaf, 256, smem, s>>>((const float *)a.X, a.d, a.d_pad, a.order,
-                                                     a.goff, a.Xb, a.nrm);
+  const unsigned grid = (unsigned)(ceil_div(a.n, kTM) + a.nleaf);
+  DRPT_CUDA(cudaFuncSetAttribute(k_leaf_mma<KP, STREAM, FP8>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_leaf_mma<KP, STREAM, FP8><<<grid, kMmaThreads, smem, s>>>(
+      tmA, tmB, a.goff, a.order, a.nrm, a.scl, a.tile_leaf, a.tile_r0, a.n_tiles, kb, a.tree,
+      a.cand_idx, a.cand_dist, a.err);
+  DRPT_LAUNCH_CHECK();
+  return DRPT_OK;
+}
+
+template <int KP>
+drpt_status mma_kp(const MixedTreeArgs &a, const CUtensorMap &tmA, const CUtensorMap &tmB, int kb,
+                   cudaStream_t s) {
+  const bool stream = kb > 4;
+  if (a.fp8)
+    return stream ? mma_t<KP, true, true>(a, tmA, tmB, kb, s) : mma_t<KP, false, true>(a, tmA, tmB, kb, s);
+  return stream ? mma_t<KP, true, false>(a, tmA, tmB, kb, s) : mma_t<KP, false, false>(a, tmA, tmB, kb, s);
+}
+
+}  // namespace
+
+// Padded row length of the mixed form's tensor-core operand: whole 128-byte
+// K blocks (64 BF16 or 128 E4M3 values).
+int mixed_d_pad(int d, int fp8) { return fp8 ? (d + 127) / 128 * 128 : (d + 63) / 64 * 64; }
+
+drpt_status launch_leaf_center(const MixedTreeArgs &a, cudaStream_t s) {
+  if (a.d % 4 != 0 || a.d > 1024 || a.d_pad != mixed_d_pad(a.d, a.fp8)) {
+    set_error("mixed mode needs d %% 4 == 0 and d <= 1024 (got %d)", a.d);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  if (a.dtype == DRPT_DTYPE_U8) center_d<uint8_t>(a, s);
+  else center_d<float>(a, s);
   DRPT_LAUNCH_CHECK();
   return DRPT_OK;
 }
 
 drpt_status launch_leaf_mma(const MixedTreeArgs &a, cudaStream_t s) {
-  if (a.d_pad % 64 != 0 || a.d_pad > 256) {
-    set_error("mixed leaf kernel: padded dimension %d unsupported (multiple of 64, <= 256)", a.d_pad);
+  const int esz = a.fp8 ? 1 : 2;
+  if ((a.d_pad * esz) % 128 != 0 || a.d_pad > 1024) {
+    set_error("mixed leaf kernel: padded dimension %d unsupported", a.d_pad);
     return DRPT_ERR_UNSUPPORTED;
   }
   k_tile_plan<<<1, 1024, 0, s>>>(a.goff, a.nleaf, a.tile_leaf, a.tile_r0, a.n_tiles);
   DRPT_LAUNCH_CHECK();
   CUtensorMap tmA, tmB;
-  DRPT_TRY(make_tmap(&tmA, a.Xb, a.n, a.d_pad, kTM));
-  DRPT_TRY(make_tmap(&tmB, a.Xb, a.n, a.d_pad, kTN));
-  const int kb = a.d_pad / 64;
-  const MmaSmem L = mma_smem_layout(kb);
-  const size_t smem = L.total + 1024;
-  const unsigned grid = (unsigned)(ceil_div(a.n, kTM) + a.nleaf);
-  if (a.kp == 16) {
-    DRPT_CUDA(cudaFuncSetAttribute(k_leaf_mma<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
-    k_leaf_mma<16><<<grid, kMmaThreads, smem, s>>>(tmA, tmB, a.goff, a.order, a.nrm, a.tile_leaf,
-                                                   a.tile_r0, a.n_tiles, kb, a.tree, a.cand_idx,
-                                                   a.cand_dist, a.err);
-  } else if (a.kp == 32) {
-    DRPT_CUDA(cudaFuncSetAttribute(k_leaf_mma<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
-    k_leaf_mma<32><<<grid, kMmaThreads, smem, s>>>(tmA, tmB, a.goff, a.order, a.nrm, a.tile_leaf,
-                                                   a.tile_r0, a.n_tiles, kb, a.tree, a.cand_idx,
-                                                   a.cand_dist, a.err);
-  } else {
-    set_error("mixed leaf kernel: %d candidates per tree unsupported (16 or 32)", a.kp);
-    return DRPT_ERR_UNSUPPORTED;
-  }
-  DRPT_LAUNCH_CHECK();
-  return DRPT_OK;
+  DRPT_TRY(make_tmap(&tmA, a.Xb, a.n, a.d_pad, kTM, a.fp8));
+  DRPT_TRY(make_tmap(&tmB, a.Xb, a.n, a.d_pad, kTN, a.fp8));
+  const int kb = a.d_pad * esz / 128;
+  if (a.kp == 16) return mma_kp<16>(a, tmA, tmB, kb, s);
+  if (a.kp == 32) return mma_kp<32>(a, tmA, tmB, kb, s);
+  set_error("mixed leaf kernel: %d candidates per tree unsupported (16 or 32)", a.kp);
+  return DRPT_ERR_UNSUPPORTED;
 }
 
 drpt_status launch_rerank(const void *X, int dtype, int d, const int32_t *visit, int64_t n,
@@ -767,8 +941,8 @@ drpt_status launch_rerank(const void *X, int dtype, int d, const int32_t *visit,
     set_error("re-rank: %d candidates for k = %d unsupported (16 or 32)", K2, k);
     return DRPT_ERR_UNSUPPORTED;
   }
-  if (d % 4 != 0 || d > 256) {
-    set_error("re-rank needs d %% 4 == 0 and d <= 256 (got %d)", d);
+  if (d % 4 != 0 || d > 1024) {
+    set_error("re-rank needs d %% 4 == 0 and d <= 1024 (got %d)", d);
     return DRPT_ERR_UNSUPPORTED;
   }
   if (dtype == DRPT_DTYPE_U8)

@@ -93,13 +93,16 @@ struct MixedTreeArgs {
   const int32_t *goff;       // this tree's leaf starts (nleaf + 1)
   int nleaf;
   int T, tree, kp;           // trees, this tree, candidates kept per point
-  __nv_bfloat16 *Xb;         // n x d_pad, centred rows in leaf order
-  float *nrm;                // n, squared norms of the BF16 rows
+  int fp8;                   // 0: BF16 tiles; 1: E4M3 tiles with per-row scales
+  void *Xb;                  // n x d_pad centred rows in leaf order (BF16 or E4M3)
+  float *nrm;                // n, squared norms of the rows the tensor cores see
+  float *scl;                // n, per-row E4M3 scales (FP8 only)
   int32_t *tile_leaf, *tile_r0, *n_tiles;  // n / 128 + nleaf
   int32_t *cand_idx;         // n x kp running list (point ids), updated tree by tree
   float *cand_dist;          // n x kp approximate squared distances, ascending
   int *err;                  // set when a bounded wait gave up
 };
+int mixed_d_pad(int d, int fp8);
 drpt_status launch_leaf_center(const MixedTreeArgs &a, cudaStream_t s);
 drpt_status launch_leaf_mma(const MixedTreeArgs &a, cudaStream_t s);
 drpt_status launch_rerank(const void *X, int dtype, int d, const int32_t *visit, int64_t n,

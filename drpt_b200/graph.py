@@ -60,13 +60,14 @@ def global_depth(n: int, tree_depth_ratio: float = 0.6, tree_depth: int = 0) -> 
 def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
                 tree_depth_ratio: float = 0.6, local_tree_offset: int = 2, tree_depth: int = 0,
                 density: float = 0.0, local_seeds=None, device: int = 0, stream=None,
-                out=None, leaf_size: int = 0):
+                out=None, leaf_size: int = 0, precision: str = "bf16"):
     """k-NN graph of `data` (n x d, uint8 or float32; a NumPy array in host
     memory or a CUDA tensor).  Returns (idx, dist, stats): idx int32 and dist
     float32 of shape (n, nn), each point's nn nearest distinct neighbours other
     than itself over all trees, ordered by (distance, index), -1/+inf padded;
     device tensors when `data` is one.  `out` = (idx, dist) preallocated
-    outputs of the same kind as `data`."""
+    outputs of the same kind as `data`.  `precision` ("bf16" or "fp8") selects
+    the operand type of the mixed form's tensor-core leaf tiles."""
     on_dev = _is_cuda_tensor(data)
     if not on_dev:
         data = np.ascontiguousarray(data)
@@ -86,6 +87,7 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
     desc.mode = {"exact": _lib.MODE_EXACT, "fast": _lib.MODE_FAST, "mixed": _lib.MODE_MIXED,
                  "fp32_leaf": _lib.MODE_FP32_LEAF}[mode]
     desc.leaf_size = leaf_size
+    desc.precision = {"bf16": _lib.PRECISION_BF16, "fp8": _lib.PRECISION_FP8_E4M3}[precision]
     desc.data_on_device = 1 if on_dev else 0
     desc.out_on_device = desc.data_on_device
     if on_dev:

@@ -63,10 +63,11 @@ typedef enum {
   DRPT_MODE_FAST = 1,
   /* Mixed-precision form: the same global trees (fast statistics), grown to
    * leaves of about `leaf_size` points; every global leaf is brute-forced
-   * with BF16 tensor-core Gram tiles (FP32 accumulation) keeping 16 (nn <= 10)
-   * or 32 candidates per tree and point; the merged 2*nn best are re-ranked
-   * with exact FP32 distances and the k-th boundary is checked in FP64.  No
-   * positional local split.  nn <= 16, d <= 256. */
+   * with BF16 (or FP8-E4M3, `precision`) tensor-core Gram tiles with FP32
+   * accumulation, keeping 16 (nn <= 10) or 32 (nn <= 32) candidates per point
+   * across the trees; those are re-ranked with FP32 distances and the k-th
+   * boundary is checked in FP64.  No positional local split.  nn <= 32,
+   * d <= 1024 and a multiple of 4. */
   DRPT_MODE_MIXED = 2,
   /* The mixed form's method in plain FP32: the same global trees and whole
    * global leaves, brute-forced with the exact sequential FP32 distance of
@@ -74,6 +75,14 @@ typedef enum {
    * equal-recall FP32 counterpart of DRPT_MODE_MIXED. */
   DRPT_MODE_FP32_LEAF = 3
 } drpt_mode;
+
+/* Operand type of the mixed form's tensor-core leaf tiles (FP32 accumulation
+ * in both cases). */
+typedef enum {
+  DRPT_PRECISION_BF16 = 0,      /* centred rows rounded to BF16 */
+  DRPT_PRECISION_FP8_E4M3 = 1   /* centred rows scaled per row to the E4M3 range
+                                   (scale = max |x - centre| / 448) and rounded */
+} drpt_precision;
 
 typedef struct drpt_ctx drpt_ctx;
 
@@ -96,7 +105,7 @@ typedef struct {
   void *stream;               /* cudaStream_t to run on; NULL = legacy default */
   int32_t leaf_size;          /* mixed and FP32-leaf modes: target global leaf
                                  size (0 = 512) */
-  int32_t reserved;
+  int32_t precision;          /* mixed mode: drpt_precision of the leaf tiles */
 } drpt_build_desc;
 
 typedef struct {

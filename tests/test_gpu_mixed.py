@@ -86,14 +86,16 @@ def test_mixed_u8_and_k16(torch):
 
 
 def test_mixed_limits_are_reported(torch):
-    X = np.random.default_rng(0).random((5000, 960), dtype=np.float32)
-    with pytest.raises(DrptError) as e:
-        build_graph(X, 2, 10, 1, mode="mixed")
-    assert e.value.status == 8
+    # d above 1,024 or not a multiple of 4, nn above 32: DRPT_ERR_UNSUPPORTED
+    for d, nn in [(1028, 10), (962, 10), (64, 33)]:
+        X = np.random.default_rng(0).random((5000, d), dtype=np.float32)
+        with pytest.raises(DrptError) as e:
+            build_graph(X, 2, nn, 1, mode="mixed")
+        assert e.value.status == 8, (d, nn)
     X = np.random.default_rng(0).random((5000, 64), dtype=np.float32)
     with pytest.raises(DrptError) as e:
-        build_graph(X, 2, 20, 1, mode="mixed")
-    assert e.value.status == 8
+        build_graph(X, 2, 10, 1, mode="mixed", precision="bf16", leaf_size=-5)
+    assert e.value.status == 1  # DRPT_ERR_INVALID_ARG
 
 
 def test_mixed_matches_its_fp32_counterpart(torch, clustered):
@@ -110,3 +112,58 @@ def test_mixed_matches_its_fp32_counterpart(torch, clustered):
     assert same >= 0.99, same
     for p in (0, 5, 999):
         assert d3[p, 0] == _exact_fp32(X[p], X[i3[p, 0]])
+
+
+def _recall(idx, q, ti):
+    return recall.recall_at_k(idx.cpu().numpy()[q], ti)
+
+
+def test_mixed_wide_rows_bf16_and_fp8(torch):
+    """d = 960 streams the operand K blocks through shared memory; nn = 20
+    keeps 32 candidates per point.  With the same trees the tensor-core forms
+    find what the exact FP32 whole-leaf form finds, in BF16 and in E4M3 with
+    per-row scales, and their output distances are FP32 distances."""
+    X = synth.anisotropic_f32(60_000, 960, n_clusters=15, seed=3)
+    Xd = torch.from_numpy(X).cuda()
+    q = recall.sample_queries(len(X), 200, seed=6)
+    ti, _ = recall.exact_knn_fp64(Xd, q, 20)
+    i3, d3, _ = build_graph(Xd, 4, 20, 7, mode="fp32_leaf", leaf_size=1024)
+    r3 = _recall(i3, q, ti)
+    d3 = d3.cpu().numpy()
+    for prec in ("bf16", "fp8"):
+        im, dm, _ = build_graph(Xd, 4, 20, 7, mode="mixed", leaf_size=1024, precision=prec)
+        torch.cuda.synchronize()
+        rm = _recall(im, q, ti)
+        assert rm >= r3 - 0.02, (prec, rm, r3)
+        I, D = im.cpu().numpy(), dm.cpu().numpy()
+        assert (d3 <= D * (1 + 2e-6)).all(), prec
+        same = np.mean([len(np.intersect1d(a, b)) / 20.0 for a, b in zip(I, i3.cpu().numpy())])
+        assert same >= 0.97, (prec, same)
+        for p in q[:10]:
+            for j in (0, 9, 19):
+                assert _close(D[p, j], X[p], X[I[p, j]]), (prec, p, j)
+
+
+def test_mixed_mnist_shaped_u8(torch):
+    """60,000 x 784 u8 (IDX3-shaped): 8 trees of whole leaves reach recall@10
+    0.85 in BF16 and in FP8."""
+    X = synth.clustered_u8(60_000, 784, seed=1)
+    Xd = torch.from_numpy(X).cuda()
+    q = recall.sample_queries(len(X), 300, seed=7)
+    ti, _ = recall.exact_knn_fp64(Xd, q, 10)
+    for prec in ("bf16", "fp8"):
+        idx, _, _ = build_graph(Xd, 8, 10, 12345, mode="mixed", leaf_size=1024, precision=prec)
+        assert _recall(idx, q, ti) >= 0.85, prec
+
+
+def test_mixed_fp8_low_dimension(torch, clustered):
+    """E4M3 at d = 128: coarser ranking than BF16, still recall@10 >= 0.85
+    with 6 trees, and the FP32 re-rank keeps the output distances exact."""
+    X, Xd = clustered
+    q = recall.sample_queries(len(X), 300, seed=8)
+    ti, _ = recall.exact_knn_fp64(Xd, q, 10)
+    idx, dist, _ = build_graph(Xd, 6, 10, 99, mode="mixed", leaf_size=1024, precision="fp8")
+    assert _recall(idx, q, ti) >= 0.85
+    I, D = idx.cpu().numpy(), dist.cpu().numpy()
+    for p in q[:10]:
+        assert _close(D[p, 0], X[p], X[I[p, 0]])
