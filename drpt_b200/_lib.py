@@ -27,6 +27,7 @@ EXPORTS = [
     "drpt_version", "drpt_last_error", "drpt_ctx_create", "drpt_ctx_destroy", "drpt_build_graph",
     "drpt_host_projection", "drpt_project", "drpt_global_trees", "drpt_local_leaves",
     "drpt_leaf_knn", "drpt_merge_candidates", "drpt_global_trees_noalloc",
+    "drpt_build_graph_batched",
 ]
 
 
@@ -48,6 +49,17 @@ class BuildDesc(ctypes.Structure):
         ("local_seeds", ctypes.POINTER(ctypes.c_uint32)), ("mode", ctypes.c_int32),
         ("data_on_device", ctypes.c_int32), ("out_on_device", ctypes.c_int32),
         ("stream", ctypes.c_void_p), ("leaf_size", ctypes.c_int32), ("precision", ctypes.c_int32),
+    ]
+
+
+class BatchDesc(ctypes.Structure):
+    _fields_ = [
+        ("nsets", ctypes.c_int32), ("d", ctypes.c_int32), ("dtype", ctypes.c_int32),
+        ("ntrees", ctypes.c_int32), ("nn", ctypes.c_int32), ("mode", ctypes.c_int32),
+        ("precision", ctypes.c_int32), ("leaf_size", ctypes.c_int32), ("seed", ctypes.c_uint32),
+        ("use_graph", ctypes.c_int32), ("density", ctypes.c_double),
+        ("data_on_device", ctypes.c_int32), ("out_on_device", ctypes.c_int32),
+        ("stream", ctypes.c_void_p),
     ]
 
 
@@ -98,6 +110,8 @@ def load(path: str = LIB_PATH):
         L.drpt_leaf_knn.argtypes = [vp, vp, i32, i64, i32, i32, vp, vp, i32, i32, vp, vp, vp]
         L.drpt_merge_candidates.argtypes = [vp, vp, vp, i64, i32, i32, vp, vp, vp]
         L.drpt_global_trees_noalloc.argtypes = [vp, i64, i32, i32, i32, vp, vp, vp, vp]
+        L.drpt_build_graph_batched.argtypes = [vp, ctypes.POINTER(BatchDesc), vp, vp, vp, vp,
+                                               ctypes.POINTER(Stats)]
         for name in EXPORTS:
             fn = getattr(L, name)
             if name not in ("drpt_version", "drpt_last_error", "drpt_ctx_destroy"):

@@ -35,6 +35,13 @@ struct drpt_ctx {
   cudaEvent_t ev[8] = {};
   std::vector<cudaEvent_t> tev;  // per-tree event pairs (mixed mode)
   int launches = 0;
+  uint64_t ws_gen = 0;           // bumped whenever a workspace buffer moves
+  // batches: the captured device work of the last graph-mode batch
+  cudaGraphExec_t gexec = nullptr;
+  cudaStream_t gstream = nullptr;  // captures and replays (the legacy stream cannot capture)
+  std::string gkey;
+  uint64_t gexec_gen = 0;
+  int glaunches = 0;
 };
 
 namespace drpt {
@@ -65,6 +72,7 @@ drpt_status ws_get(drpt_ctx *c, const char *name, size_t count, T **out) {
       return DRPT_ERR_OOM;
     }
     b.bytes = bytes;
+    ++c->ws_gen;
   }
   *out = (T *)b.p;
   return DRPT_OK;
@@ -336,6 +344,83 @@ drpt_status leaf_depth(int64_t n, int leaf_size_in, int *gd_out) {
   return DRPT_OK;
 }
 
+// Leaf phase of the mixed form over the global leaves of T trees (`order`,
+// `goff`: T x n and T x (nleaf + 1)): per tree K8 centring and K10
+// tensor-core brute force into the running candidate lists, then K11 re-rank
+// into oi / od.  Kernel launches only (no host synchronisation), so the
+// batched path can capture it in a CUDA graph; `timed` records the per-tree
+// events that the stats report.  mixed_check reads the kernels' error flag.
+drpt_status mixed_leaf_phase(drpt_ctx *c, const void *X, int dtype, int64_t n, int d, int T,
+                             int nn, int fp8, const int32_t *order, const int32_t *goff,
+                             int nleaf, int32_t *oi, float *od, bool timed, cudaStream_t s) {
+  const int d_pad = mixed_d_pad(d, fp8);
+  const int kp = nn <= 10 ? 16 : 32;  // running candidates per point, re-ranked at the end
+  cudaEvent_t *ev = c->ev;
+  MixedTreeArgs a{};
+  a.X = X;
+  a.dtype = dtype;
+  a.n = n;
+  a.d = d;
+  a.d_pad = d_pad;
+  a.nleaf = nleaf;
+  a.T = T;
+  a.kp = kp;
+  a.fp8 = fp8;
+  uint8_t *xb = nullptr;
+  DRPT_TRY(ws_get(c, "mx_xb", (size_t)n * d_pad * (fp8 ? 1 : 2), &xb));
+  a.Xb = xb;
+  DRPT_TRY(ws_get(c, "mx_nrm", (size_t)n, &a.nrm));
+  DRPT_TRY(ws_get(c, "mx_scl", fp8 ? (size_t)n : 1, &a.scl));
+  const size_t tiles = (size_t)ceil_div(n, 128) + nleaf;
+  DRPT_TRY(ws_get(c, "mx_tile_leaf", tiles, &a.tile_leaf));
+  DRPT_TRY(ws_get(c, "mx_tile_r0", tiles, &a.tile_r0));
+  DRPT_TRY(ws_get(c, "mx_n_tiles", 1, &a.n_tiles));
+  DRPT_TRY(ws_get(c, "mx_err", 1, &a.err));
+  DRPT_TRY(ws_get(c, "mx_run_idx", (size_t)n * kp, &a.cand_idx));
+  DRPT_TRY(ws_get(c, "mx_run_dist", (size_t)n * kp, &a.cand_dist));
+  DRPT_CUDA(cudaMemsetAsync(a.err, 0, sizeof(int), s));
+  if (timed) {
+    DRPT_CUDA(cudaEventRecord(ev[3], s));
+    while ((int)c->tev.size() < 3 * T) {
+      cudaEvent_t e;
+      DRPT_CUDA(cudaEventCreate(&e));
+      c->tev.push_back(e);
+    }
+  }
+  for (int t = 0; t < T; ++t) {
+    a.tree = t;
+    a.order = order + (size_t)t * n;
+    a.goff = goff + (size_t)t * (nleaf + 1);
+    if (timed) DRPT_CUDA(cudaEventRecord(c->tev[3 * t], s));
+    DRPT_TRY(launch_leaf_center(a, s));
+    if (timed) DRPT_CUDA(cudaEventRecord(c->tev[3 * t + 1], s));
+    DRPT_TRY(launch_leaf_mma(a, s));
+    if (timed) DRPT_CUDA(cudaEventRecord(c->tev[3 * t + 2], s));
+    c->launches += 3;
+  }
+  if (timed) DRPT_CUDA(cudaEventRecord(ev[4], s));
+  // Re-rank in the leaf order of the last tree: a point's candidates are
+  // mostly its leaf-mates there, so their rows stay in L2.
+  DRPT_TRY(launch_rerank(X, dtype, d, order + (size_t)(T - 1) * n, n, a.cand_idx, kp, nn, oi,
+                         od, s));
+  c->launches += 1;
+  if (timed) DRPT_CUDA(cudaEventRecord(ev[5], s));
+  return DRPT_OK;
+}
+
+drpt_status mixed_check(drpt_ctx *c, cudaStream_t s) {
+  int *err_d = nullptr;
+  DRPT_TRY(ws_get(c, "mx_err", 1, &err_d));
+  int err = 0;
+  DRPT_CUDA(cudaMemcpyAsync(&err, err_d, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DRPT_CUDA(cudaStreamSynchronize(s));
+  if (err) {
+    set_error("a bounded wait in the tensor-core leaf kernel gave up");
+    return DRPT_ERR_TIMEOUT;
+  }
+  return DRPT_OK;
+}
+
 // Mixed-precision pipeline (DRPT_MODE_MIXED): global trees with fast
 // statistics grown to leaves of about `leaf_size` points, BF16 tensor-core
 // brute force of every global leaf, cross-tree merge of the approximate
@@ -357,11 +442,9 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
     set_error("mixed mode supports d %% 4 == 0 and d <= 1024 (got %d)", d);
     return DRPT_ERR_UNSUPPORTED;
   }
-  const int d_pad = mixed_d_pad(d, fp8);
   int gd = 0;
   DRPT_TRY(leaf_depth(n, desc->leaf_size, &gd));
   const int nleaf = 1 << (gd - 1);
-  const int kp = nn <= 10 ? 16 : 32;  // running candidates per point, re-ranked at the end
   const int L = gd * T;
   const float density = (float)(desc->density == 0 ? 1.0 / std::sqrt((double)d) : desc->density);
   cudaEvent_t *ev = c->ev;
@@ -380,60 +463,9 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
   DRPT_TRY(global_trees(c, P, n, T, gd, 0, nullptr, &order, &goff, s));
   DRPT_CUDA(cudaEventRecord(ev[2], s));
 
-  MixedTreeArgs a{};
-  a.X = X;
-  a.dtype = desc->dtype;
-  a.n = n;
-  a.d = d;
-  a.d_pad = d_pad;
-  a.nleaf = nleaf;
-  a.T = T;
-  a.kp = kp;
-  a.fp8 = fp8;
-  uint8_t *xb = nullptr;
-  DRPT_TRY(ws_get(c, "mx_xb", (size_t)n * d_pad * (fp8 ? 1 : 2), &xb));
-  a.Xb = xb;
-  DRPT_TRY(ws_get(c, "mx_nrm", (size_t)n, &a.nrm));
-  DRPT_TRY(ws_get(c, "mx_scl", fp8 ? (size_t)n : 1, &a.scl));
-  const size_t tiles = (size_t)ceil_div(n, 128) + nleaf;
-  DRPT_TRY(ws_get(c, "mx_tile_leaf", tiles, &a.tile_leaf));
-  DRPT_TRY(ws_get(c, "mx_tile_r0", tiles, &a.tile_r0));
-  DRPT_TRY(ws_get(c, "mx_n_tiles", 1, &a.n_tiles));
-  DRPT_TRY(ws_get(c, "mx_err", 1, &a.err));
-  DRPT_TRY(ws_get(c, "mx_run_idx", (size_t)n * kp, &a.cand_idx));
-  DRPT_TRY(ws_get(c, "mx_run_dist", (size_t)n * kp, &a.cand_dist));
-  DRPT_CUDA(cudaMemsetAsync(a.err, 0, sizeof(int), s));
-  DRPT_CUDA(cudaEventRecord(ev[3], s));
-  while ((int)c->tev.size() < 3 * T) {
-    cudaEvent_t e;
-    DRPT_CUDA(cudaEventCreate(&e));
-    c->tev.push_back(e);
-  }
-  for (int t = 0; t < T; ++t) {
-    a.tree = t;
-    a.order = order + (size_t)t * n;
-    a.goff = goff + (size_t)t * (nleaf + 1);
-    DRPT_CUDA(cudaEventRecord(c->tev[3 * t], s));
-    DRPT_TRY(launch_leaf_center(a, s));
-    DRPT_CUDA(cudaEventRecord(c->tev[3 * t + 1], s));
-    DRPT_TRY(launch_leaf_mma(a, s));
-    DRPT_CUDA(cudaEventRecord(c->tev[3 * t + 2], s));
-    c->launches += 3;
-  }
-  DRPT_CUDA(cudaEventRecord(ev[4], s));
-  // Re-rank in the leaf order of the last tree: a point's candidates are
-  // mostly its leaf-mates there, so their rows stay in L2.
-  DRPT_TRY(launch_rerank(X, desc->dtype, d, order + (size_t)(T - 1) * n, n, a.cand_idx, kp, nn, oi,
-                         od, s));
-  c->launches += 1;
-  DRPT_CUDA(cudaEventRecord(ev[5], s));
-  int err = 0;
-  DRPT_CUDA(cudaMemcpyAsync(&err, a.err, sizeof(int), cudaMemcpyDeviceToHost, s));
-  DRPT_CUDA(cudaStreamSynchronize(s));
-  if (err) {
-    set_error("a bounded wait in the tensor-core leaf kernel gave up");
-    return DRPT_ERR_TIMEOUT;
-  }
+  DRPT_TRY(mixed_leaf_phase(c, X, desc->dtype, n, d, T, nn, fp8, order, goff, nleaf, oi, od,
+                            /*timed=*/true, s));
+  DRPT_TRY(mixed_check(c, s));
   if (stats) {
     std::memset(stats, 0, sizeof(*stats));
     stats->tree_depth = gd;
@@ -544,6 +576,241 @@ drpt_status run_fp32_leaf(drpt_ctx *c, const drpt_build_desc *desc, const void *
   return DRPT_OK;
 }
 
+
+// ---------------------------------------------------------------- batches
+// A batch is built as one forest.  Its first level is virtual: level l0 =
+// ceil(log2(nsets)) of every tree holds the datasets as its 2^l0 root slots
+// (slots past nsets are empty), the points in index order.  The level
+// kernels then split every slot exactly as a build of that dataset alone
+// would split its root (same node-aligned statistics, median and stable
+// partition), and a dataset of global depth gd_s stops splitting after
+// gd_s - 1 levels (its nodes keep all points below that).  Dataset s projects
+// with the matrix its own build would draw (d x gd_s*T from the seed), so
+// every dataset's trees, leaves and lists equal its single build's.
+struct BatchPlan {
+  int nsets = 0, l0 = 0, gdm = 0, nleaf = 0, T = 0, nn = 0, d = 0, dtype = 0, fp8 = 0, mode = 0;
+  int64_t n = 0;
+  int ncols = 0;                 // T * (gdm - 1) projected columns
+  CscDev csc{};
+  int32_t *root_off = nullptr;   // T x (2^l0 + 1)
+  int8_t *stop = nullptr;        // 2^l0
+  int64_t *set_off = nullptr;    // nsets + 1
+  float *P = nullptr;
+  int32_t *ord[2] = {}, *off[2] = {};
+  float *val[2] = {};
+  TreeLevelArgs lv{};
+  int32_t *order = nullptr, *goff = nullptr;  // final leaves
+  int32_t *cidx = nullptr;       // fp32_leaf candidates
+  float *cdist = nullptr;
+};
+
+drpt_status batch_prepare(drpt_ctx *c, const drpt_batch_desc *desc, const int64_t *offs,
+                          BatchPlan *bp, cudaStream_t s) {
+  const int nsets = desc->nsets, T = desc->ntrees, d = desc->d;
+  const int64_t n = offs[nsets];
+  bp->nsets = nsets;
+  bp->T = T;
+  bp->nn = desc->nn;
+  bp->d = d;
+  bp->dtype = desc->dtype;
+  bp->mode = desc->mode;
+  bp->fp8 = desc->precision == DRPT_PRECISION_FP8_E4M3;
+  bp->n = n;
+  std::vector<int> gds(nsets);
+  int gdm = 2;  // at least one level runs, even if no dataset splits
+  for (int i = 0; i < nsets; ++i) {
+    DRPT_TRY(leaf_depth(offs[i + 1] - offs[i], desc->leaf_size, &gds[i]));
+    gdm = std::max(gdm, gds[i]);
+  }
+  int l0 = 0;
+  while ((1 << l0) < nsets) ++l0;
+  bp->l0 = l0;
+  bp->gdm = gdm;
+  if (l0 + gdm - 1 > 24 || ((int64_t)T << (l0 + gdm - 2)) > (1 << 20)) {
+    set_error("batch of %d datasets needs %d tree levels: too many nodes", nsets, l0 + gdm - 1);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  const int nroot = 1 << l0;
+  bp->nleaf = 1 << (l0 + gdm - 1);
+  // projection: one column set per distinct global depth
+  const int ncols = T * (gdm - 1);
+  bp->ncols = ncols;
+  const float density = (float)(desc->density == 0 ? 1.0 / std::sqrt((double)d) : desc->density);
+  std::map<int, int> set_of_depth;
+  std::vector<int32_t> colptr, row;
+  std::vector<float> val;
+  for (int i = 0; i < nsets; ++i) {
+    if (set_of_depth.count(gds[i])) continue;
+    const int g = gds[i], cs = (int)set_of_depth.size();
+    set_of_depth[g] = cs;
+    const int L = g * T;
+    std::vector<float> B((size_t)d * L);
+    host_projection_matrix(desc->seed, d, L, density, B.data());
+    colptr.push_back((int32_t)row.size());
+    for (int t = 0; t < T; ++t)
+      for (int l = 0; l + 1 < gdm; ++l) {
+        if (l + 1 < g)  // levels the dataset splits on; the others project to 0
+          for (int k = 0; k < d; ++k) {
+            const float b = B[(int64_t)k * L + t * g + l];
+            if (b != 0.0f) {
+              row.push_back(k);
+              val.push_back(b);
+            }
+          }
+        colptr.push_back((int32_t)row.size());
+      }
+  }
+  const int pts = project_points_per_block(d);
+  std::vector<int32_t> blocks;
+  for (int i = 0; i < nsets; ++i)
+    for (int64_t r = offs[i]; r < offs[i + 1]; r += pts) {
+      blocks.push_back((int32_t)r);
+      blocks.push_back((int32_t)std::min<int64_t>(pts, offs[i + 1] - r));
+      blocks.push_back(set_of_depth[gds[i]]);
+    }
+  int32_t *dcol, *drow, *dblk;
+  float *dval;
+  DRPT_TRY(ws_get(c, "bt_colptr", colptr.size(), &dcol));
+  DRPT_TRY(ws_get(c, "bt_row", std::max<size_t>(row.size(), 1), &drow));
+  DRPT_TRY(ws_get(c, "bt_val", std::max<size_t>(val.size(), 1), &dval));
+  DRPT_TRY(ws_get(c, "bt_blocks", std::max<size_t>(blocks.size(), 1), &dblk));
+  // root slots, stop depths and dataset offsets
+  std::vector<int32_t> ro((size_t)T * (nroot + 1));
+  for (int t = 0; t < T; ++t)
+    for (int j = 0; j <= nroot; ++j)
+      ro[(size_t)t * (nroot + 1) + j] = (int32_t)offs[std::min(j, nsets)];
+  std::vector<int8_t> stop(nroot, 0);
+  for (int i = 0; i < nsets; ++i) stop[i] = (int8_t)(gds[i] - 1);
+  DRPT_TRY(ws_get(c, "bt_root_off", ro.size(), &bp->root_off));
+  DRPT_TRY(ws_get(c, "bt_stop", stop.size(), &bp->stop));
+  DRPT_TRY(ws_get(c, "bt_set_off", (size_t)nsets + 1, &bp->set_off));
+  // every other buffer of the build, sized now so that a captured run
+  // allocates nothing
+  DRPT_TRY(ws_get(c, "P", std::max<size_t>(ncols, 1) * n, &bp->P));
+  DRPT_TRY(ws_get(c, "ord_a", (size_t)T * n, &bp->ord[0]));
+  DRPT_TRY(ws_get(c, "ord_b", (size_t)T * n, &bp->ord[1]));
+  DRPT_TRY(ws_get(c, "val_a", (size_t)T * n, &bp->val[0]));
+  DRPT_TRY(ws_get(c, "val_b", (size_t)T * n, &bp->val[1]));
+  DRPT_TRY(ws_get(c, "off_a", (size_t)T * (bp->nleaf + 1), &bp->off[0]));
+  DRPT_TRY(ws_get(c, "off_b", (size_t)T * (bp->nleaf + 1), &bp->off[1]));
+  const int last = l0 + gdm - 2;
+  const int64_t Gmax = (int64_t)T << last;
+  const int64_t Umax = tree_level_max_units(n, T, last);
+  TreeLevelArgs &a = bp->lv;
+  DRPT_TRY(ws_get(c, "lv_node_ubase", Gmax + 1, &a.node_ubase));
+  DRPT_TRY(ws_get(c, "lv_unit_node", Umax, &a.unit_node));
+  DRPT_TRY(ws_get(c, "lv_unit_lo", Umax, &a.unit_lo));
+  DRPT_TRY(ws_get(c, "lv_n_units", 1, &a.n_units));
+  DRPT_TRY(ws_get(c, "lv_node_D", Gmax * kBins, &a.node_D));
+  DRPT_TRY(ws_get(c, "lv_unit_s", 2 * Umax, &a.unit_s));
+  DRPT_TRY(ws_get(c, "lv_unit_hist", Umax * kBins, &a.unit_hist));
+  DRPT_TRY(ws_get(c, "lv_node_med", Gmax, &a.node_med));
+  DRPT_TRY(ws_get(c, "lv_unit_left", Umax, &a.unit_left));
+  DRPT_TRY(ws_get(c, "lv_unit_lbase", Umax, &a.unit_lbase));
+  DRPT_TRY(ws_get(c, "lv_node_nleft", Gmax, &a.node_nleft));
+  if (bp->mode == DRPT_MODE_MIXED) {
+    const int d_pad = mixed_d_pad(d, bp->fp8), kp = bp->nn <= 10 ? 16 : 32;
+    const size_t tiles = (size_t)ceil_div(n, 128) + bp->nleaf;
+    uint8_t *u8p;
+    int32_t *i32p;
+    float *f32p;
+    int *ip;
+    DRPT_TRY(ws_get(c, "mx_xb", (size_t)n * d_pad * (bp->fp8 ? 1 : 2), &u8p));
+    DRPT_TRY(ws_get(c, "mx_nrm", (size_t)n, &f32p));
+    DRPT_TRY(ws_get(c, "mx_scl", bp->fp8 ? (size_t)n : 1, &f32p));
+    DRPT_TRY(ws_get(c, "mx_tile_leaf", tiles, &i32p));
+    DRPT_TRY(ws_get(c, "mx_tile_r0", tiles, &i32p));
+    DRPT_TRY(ws_get(c, "mx_n_tiles", 1, &i32p));
+    DRPT_TRY(ws_get(c, "mx_err", 1, &ip));
+    DRPT_TRY(ws_get(c, "mx_run_idx", (size_t)n * kp, &i32p));
+    DRPT_TRY(ws_get(c, "mx_run_dist", (size_t)n * kp, &f32p));
+  } else {
+    DRPT_TRY(ws_get(c, "cand_idx", (size_t)n * T * bp->nn, &bp->cidx));
+    DRPT_TRY(ws_get(c, "cand_dist", (size_t)n * T * bp->nn, &bp->cdist));
+  }
+  // uploads (pageable sources: complete before the calls return)
+  DRPT_CUDA(cudaMemcpyAsync(dcol, colptr.data(), colptr.size() * 4, cudaMemcpyHostToDevice, s));
+  if (!row.empty()) {
+    DRPT_CUDA(cudaMemcpyAsync(drow, row.data(), row.size() * 4, cudaMemcpyHostToDevice, s));
+    DRPT_CUDA(cudaMemcpyAsync(dval, val.data(), val.size() * 4, cudaMemcpyHostToDevice, s));
+  }
+  DRPT_CUDA(cudaMemcpyAsync(dblk, blocks.data(), blocks.size() * 4, cudaMemcpyHostToDevice, s));
+  DRPT_CUDA(cudaMemcpyAsync(bp->root_off, ro.data(), ro.size() * 4, cudaMemcpyHostToDevice, s));
+  DRPT_CUDA(cudaMemcpyAsync(bp->stop, stop.data(), stop.size(), cudaMemcpyHostToDevice, s));
+  DRPT_CUDA(cudaMemcpyAsync(bp->set_off, offs, ((size_t)nsets + 1) * 8, cudaMemcpyHostToDevice, s));
+  bp->csc = CscDev{dcol, drow, dval, ncols};
+  bp->csc.blocks = dblk;
+  bp->csc.nblocks = (int32_t)(blocks.size() / 3);
+  // the leaf arrays the level loop ends in
+  const int fin = (gdm - 1) & 1;
+  bp->order = bp->ord[fin];
+  bp->goff = bp->off[fin];
+  return DRPT_OK;
+}
+
+// The batch's device work: kernel launches and device-side memsets only, so
+// that it can be captured in a CUDA graph.
+drpt_status batch_enqueue(drpt_ctx *c, const BatchPlan &bp, const void *X, int32_t *oi,
+                          float *od, bool timed, cudaStream_t s) {
+  const int64_t n = bp.n;
+  const int T = bp.T;
+  if (bp.ncols > 0) {
+    DRPT_TRY(launch_project(X, bp.dtype, n, bp.d, bp.csc, bp.P, s));
+    c->launches += 1;
+  }
+  TreeLevelArgs a = bp.lv;
+  a.P = bp.P;
+  a.n = n;
+  a.T = T;
+  a.gd = bp.gdm;
+  a.p_level0 = bp.l0;
+  a.stop = bp.stop;
+  a.medians = nullptr;
+  a.exact = 0;
+  int cur = 0;
+  for (int k = 0; k < bp.gdm - 1; ++k) {
+    a.level = bp.l0 + k;
+    a.ord_in = k == 0 ? nullptr : bp.ord[cur];  // index order at the root slots
+    a.val_in = k == 0 ? nullptr : bp.val[cur];  // read from P at the root slots
+    a.off_in = k == 0 ? bp.root_off : bp.off[cur];
+    a.ord_out = bp.ord[cur ^ 1];
+    a.val_out = k + 1 < bp.gdm - 1 ? bp.val[cur ^ 1] : nullptr;
+    a.off_out = bp.off[cur ^ 1];
+    DRPT_TRY(launch_tree_level(a, tree_level_max_units(n, T, a.level), s));
+    c->launches += tree_level_kernels(0);
+    cur ^= 1;
+  }
+  if (timed) DRPT_CUDA(cudaEventRecord(c->ev[2], s));
+  if (bp.mode == DRPT_MODE_MIXED) {
+    DRPT_TRY(mixed_leaf_phase(c, X, bp.dtype, n, bp.d, T, bp.nn, bp.fp8, bp.order, bp.goff,
+                              bp.nleaf, oi, od, timed, s));
+  } else {
+    if (timed) DRPT_CUDA(cudaEventRecord(c->ev[3], s));
+    LeafKnnArgs ka{X, bp.dtype, n, bp.d, T, bp.nn, bp.order, bp.goff, bp.nleaf, bp.cidx, bp.cdist};
+    DRPT_TRY(launch_leaf_knn_exact(ka, s));
+    c->launches += leaf_knn_exact_kernels();
+    if (timed) DRPT_CUDA(cudaEventRecord(c->ev[4], s));
+    DRPT_TRY(launch_merge(bp.cidx, bp.cdist, n, T, bp.nn, bp.nn, oi, od, s));
+    c->launches += 1;
+    if (timed) DRPT_CUDA(cudaEventRecord(c->ev[5], s));
+  }
+  DRPT_TRY(launch_localize(oi, n, bp.nn, bp.set_off, bp.nsets, s));
+  c->launches += 1;
+  return DRPT_OK;
+}
+
+std::string batch_key(const drpt_batch_desc *d, const int64_t *offs, const void *X,
+                      const void *oi, const void *od) {
+  std::string k;
+  auto put = [&](const void *p, size_t b) { k.append(static_cast<const char *>(p), b); };
+  put(d, sizeof(*d));
+  put(offs, ((size_t)d->nsets + 1) * sizeof(int64_t));
+  put(&X, sizeof(X));
+  put(&oi, sizeof(oi));
+  put(&od, sizeof(od));
+  return k;
+}
+
 }  // namespace
 }  // namespace drpt
 
@@ -588,7 +855,151 @@ void drpt_ctx_destroy(drpt_ctx *c) {
     if (e) cudaEventDestroy(e);
   for (auto &e : c->tev)
     if (e) cudaEventDestroy(e);
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  if (c->gstream) cudaStreamDestroy(c->gstream);
   delete c;
+}
+
+drpt_status drpt_build_graph_batched(drpt_ctx *c, const drpt_batch_desc *desc,
+                                     const int64_t *offsets, const void *data, int32_t *out_idx,
+                                     float *out_dist, drpt_stats *stats) {
+  if (!c || !desc || !offsets || !data || !out_idx) return DRPT_ERR_INVALID_ARG;
+  const int nsets = desc->nsets;
+  if (nsets < 1 || nsets > 65536 || desc->d <= 0 || desc->ntrees <= 0 || desc->nn <= 0 ||
+      desc->nn > kMaxK || (desc->dtype != DRPT_DTYPE_F32 && desc->dtype != DRPT_DTYPE_U8) ||
+      (desc->mode != DRPT_MODE_MIXED && desc->mode != DRPT_MODE_FP32_LEAF) ||
+      (desc->precision != DRPT_PRECISION_BF16 && desc->precision != DRPT_PRECISION_FP8_E4M3)) {
+    set_error("invalid batch descriptor");
+    return DRPT_ERR_INVALID_ARG;
+  }
+  if (offsets[0] != 0) {
+    set_error("offsets[0] must be 0");
+    return DRPT_ERR_INVALID_ARG;
+  }
+  for (int i = 0; i < nsets; ++i)
+    if (offsets[i + 1] - offsets[i] < 2) {
+      set_error("dataset %d has %lld rows (at least 2 needed)", i,
+                (long long)(offsets[i + 1] - offsets[i]));
+      return DRPT_ERR_INVALID_ARG;
+    }
+  const int64_t n = offsets[nsets];
+  const int d = desc->d, nn = desc->nn;
+  if (n > INT32_MAX) {
+    set_error("batch of %lld rows: at most 2^31 - 1", (long long)n);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  if (desc->mode == DRPT_MODE_MIXED && (nn > 32 || d % 4 != 0 || d > 1024)) {
+    set_error("mixed mode supports nn <= 32 and d %% 4 == 0, d <= 1024 (got nn %d, d %d)", nn, d);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  if (desc->use_graph && (!desc->data_on_device || !desc->out_on_device)) {
+    set_error("graph mode needs device input and output pointers");
+    return DRPT_ERR_INVALID_ARG;
+  }
+  DRPT_CUDA(cudaSetDevice(c->device));
+  cudaStream_t s = (cudaStream_t)desc->stream;
+  cudaEvent_t *ev = c->ev;
+  const size_t esz = desc->dtype == DRPT_DTYPE_U8 ? 1 : 4;
+  const int launches0 = c->launches;
+
+  // graph replay
+  std::string key;
+  if (desc->use_graph) {
+    key = batch_key(desc, offsets, data, out_idx, out_dist);
+    if (!c->gstream) DRPT_CUDA(cudaStreamCreateWithFlags(&c->gstream, cudaStreamNonBlocking));
+    if (c->gexec && c->gkey == key && c->gexec_gen == c->ws_gen) {
+      // replay on the context's stream, ordered after and before the caller's
+      DRPT_CUDA(cudaEventRecord(ev[0], s));
+      DRPT_CUDA(cudaStreamWaitEvent(c->gstream, ev[0], 0));
+      DRPT_CUDA(cudaGraphLaunch(c->gexec, c->gstream));
+      DRPT_CUDA(cudaEventRecord(ev[7], c->gstream));
+      DRPT_CUDA(cudaStreamWaitEvent(s, ev[7], 0));
+      DRPT_CUDA(cudaEventRecord(ev[6], s));
+      if (desc->mode == DRPT_MODE_MIXED) DRPT_TRY(mixed_check(c, s));
+      DRPT_CUDA(cudaEventSynchronize(ev[6]));
+      c->launches += c->glaunches;
+      if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->kernels_launched = c->glaunches;
+        stats->ms_total = elapsed(ev[0], ev[6]);
+      }
+      return DRPT_OK;
+    }
+    if (c->gexec) {
+      cudaGraphExecDestroy(c->gexec);
+      c->gexec = nullptr;
+    }
+  }
+
+  DRPT_CUDA(cudaEventRecord(ev[0], s));
+  const void *X = data;
+  if (!desc->data_on_device) {
+    void *xd;
+    DRPT_TRY(ws_get(c, "x", (size_t)n * d * esz, (uint8_t **)&xd));
+    DRPT_CUDA(cudaMemcpyAsync(xd, data, (size_t)n * d * esz, cudaMemcpyHostToDevice, s));
+    X = xd;
+  }
+  int32_t *oi = out_idx;
+  float *od = out_dist;
+  if (!desc->out_on_device) {
+    DRPT_TRY(ws_get(c, "out_idx", (size_t)n * nn, &oi));
+    DRPT_TRY(ws_get(c, "out_dist", (size_t)n * nn, &od));
+  } else if (!od) {
+    DRPT_TRY(ws_get(c, "out_dist", (size_t)n * nn, &od));
+  }
+  BatchPlan bp;
+  DRPT_TRY(batch_prepare(c, desc, offsets, &bp, s));
+  DRPT_CUDA(cudaEventRecord(ev[1], s));
+  DRPT_TRY(batch_enqueue(c, bp, X, oi, od, /*timed=*/true, s));
+  if (!desc->out_on_device) {
+    DRPT_CUDA(cudaMemcpyAsync(out_idx, oi, (size_t)n * nn * 4, cudaMemcpyDeviceToHost, s));
+    if (out_dist)
+      DRPT_CUDA(cudaMemcpyAsync(out_dist, od, (size_t)n * nn * 4, cudaMemcpyDeviceToHost, s));
+  }
+  DRPT_CUDA(cudaEventRecord(ev[6], s));
+  if (desc->mode == DRPT_MODE_MIXED) DRPT_TRY(mixed_check(c, s));
+  DRPT_CUDA(cudaEventSynchronize(ev[6]));
+  const int launched = c->launches - launches0;
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->tree_depth = bp.l0 + bp.gdm;
+    stats->global_depth = bp.gdm;
+    stats->n_global_leaves = bp.nleaf;
+    stats->n_final_leaves = bp.nleaf;
+    stats->kernels_launched = launched;
+    stats->ms_project = elapsed(ev[0], ev[1]);
+    stats->ms_global = elapsed(ev[1], ev[2]);
+    stats->ms_leaf_knn = elapsed(ev[3], ev[4]);
+    stats->ms_merge = elapsed(ev[4], ev[5]);
+    stats->ms_total = elapsed(ev[0], ev[6]);
+    if (desc->mode == DRPT_MODE_MIXED)
+      for (int t = 0; t < bp.T; ++t) {
+        stats->ms_leaf_stage += elapsed(c->tev[3 * t], c->tev[3 * t + 1]);
+        stats->ms_leaf_mma += elapsed(c->tev[3 * t + 1], c->tev[3 * t + 2]);
+      }
+  }
+  if (desc->use_graph) {
+    // capture the device work of this batch for the next calls (every
+    // buffer is sized already, so the captured launches allocate nothing)
+    const int l0 = c->launches;
+    cudaGraph_t g = nullptr;
+    DRPT_CUDA(cudaStreamBeginCapture(c->gstream, cudaStreamCaptureModeThreadLocal));
+    const drpt_status st = batch_enqueue(c, bp, X, oi, od, /*timed=*/false, c->gstream);
+    const cudaError_t ce = cudaStreamEndCapture(c->gstream, &g);
+    if (st != DRPT_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    DRPT_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&c->gexec, g, 0);
+    cudaGraphDestroy(g);
+    DRPT_CUDA(ie);
+    c->gkey = key;
+    c->gexec_gen = c->ws_gen;
+    c->glaunches = c->launches - l0;
+    c->launches = l0;
+  }
+  return DRPT_OK;
 }
 
 drpt_status drpt_host_projection(uint32_t seed, int32_t d, int32_t L, float density, float *B) {

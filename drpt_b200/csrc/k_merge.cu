@@ -141,3 +141,38 @@ drpt_status launch_merge(const int32_t *cand_idx, const float *cand_dist, int64_
 }
 
 }  // namespace drpt
+
+namespace drpt {
+namespace {
+
+// Batches: point p of dataset s (rows [off[s], off[s+1])) gets its
+// neighbours' ids relative to off[s].
+__global__ void k_localize(int32_t *__restrict__ idx, int64_t n, int k,
+                           const int64_t *__restrict__ off, int nsets) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  int lo = 0, hi = nsets;  // largest s with off[s] <= p
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(off + mid) <= p) lo = mid;
+    else hi = mid;
+  }
+  const int32_t base = (int32_t)__ldg(off + lo);
+  int32_t *row = idx + p * k;
+  for (int j = 0; j < k; ++j) {
+    const int32_t v = row[j];
+    if (v >= 0) row[j] = v - base;
+  }
+}
+
+}  // namespace
+
+drpt_status launch_localize(int32_t *idx, int64_t n, int k, const int64_t *set_off, int nsets,
+                            cudaStream_t s) {
+  if (n <= 0) return DRPT_OK;
+  k_localize<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(idx, n, k, set_off, nsets);
+  DRPT_LAUNCH_CHECK();
+  return DRPT_OK;
+}
+
+}  // namespace drpt

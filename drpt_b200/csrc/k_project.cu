@@ -18,14 +18,21 @@ constexpr int kThreads = 256;
 template <typename T>
 __device__ __forceinline__ float to_f(T v) { return (float)v; }
 
-// Block: `pts` consecutive points; thread pairs (point, column) with the
-// point index fastest so a warp writes 32 consecutive P entries of a column.
+// Block: `pts` consecutive points (or the block table's entry: first point,
+// points, column set); thread pairs (point, column) with the point index
+// fastest so a warp writes 32 consecutive P entries of a column.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_project(const T *__restrict__ X, int64_t n, int d,
                                                       CscDev csc, float *__restrict__ P, int pts) {
   extern __shared__ float xs[];  // pts x (d + 1), padded against bank conflicts
-  const int64_t p0 = (int64_t)blockIdx.x * pts;
-  const int np = (int)min64(pts, n - p0);
+  int64_t p0 = (int64_t)blockIdx.x * pts;
+  int np = (int)min64(pts, n - p0);
+  if (csc.blocks) {
+    const int32_t *b = csc.blocks + 3 * (int64_t)blockIdx.x;
+    p0 = b[0];
+    np = b[1];
+    csc.colptr += (int64_t)b[2] * (csc.ncols + 1);
+  }
   const int ld = d + 1;
   // Stage the rows: consecutive threads read consecutive elements of a row.
   const int total = np * d;
@@ -48,18 +55,22 @@ __global__ void __launch_bounds__(kThreads) k_project(const T *__restrict__ X, i
 
 }  // namespace
 
+int project_points_per_block(int d) {
+  // About 96 KB of staged rows per block, at least 8 and at most 128 points.
+  const int pts = (int)(96 * 1024 / ((d + 1) * (int)sizeof(float)));
+  return pts < 8 ? 8 : (pts > 128 ? 128 : pts);
+}
+
 drpt_status launch_project(const void *X, int dtype, int64_t n, int d, const CscDev &csc,
                            float *P, cudaStream_t s) {
   if (n <= 0 || csc.ncols <= 0) return DRPT_OK;
-  // About 96 KB of staged rows per block, at least 8 and at most 128 points.
-  int pts = (int)(96 * 1024 / ((d + 1) * (int)sizeof(float)));
-  pts = pts < 8 ? 8 : (pts > 128 ? 128 : pts);
+  const int pts = project_points_per_block(d);
   const size_t smem = (size_t)pts * (d + 1) * sizeof(float);
   if (smem > 227 * 1024) {
     set_error("projection: d = %d too large for one staged row block", d);
     return DRPT_ERR_UNSUPPORTED;
   }
-  const unsigned grid = (unsigned)ceil_div(n, pts);
+  const unsigned grid = csc.blocks ? (unsigned)csc.nblocks : (unsigned)ceil_div(n, pts);
   if (dtype == DRPT_DTYPE_U8) {
     DRPT_CUDA(cudaFuncSetAttribute(k_project<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));

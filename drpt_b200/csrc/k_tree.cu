@@ -113,8 +113,10 @@ __device__ __forceinline__ NodeRange node_range(const TreeLevelArgs &a, int g) {
 }
 
 __device__ __forceinline__ const float *tree_vals(const TreeLevelArgs &a, int t) {
-  // Level 0 reads the root values straight from P (column t*(gd-1)).
-  return a.level == 0 ? a.P + (int64_t)t * (a.gd - 1) * a.n : a.val_in + (int64_t)t * a.n;
+  // The first level (p_level0) reads its values straight from P (column
+  // t*(gd-1)): the points are still in index order there.
+  return a.level == a.p_level0 ? a.P + (int64_t)t * (a.gd - 1) * a.n
+                               : a.val_in + (int64_t)t * a.n;
 }
 
 // ------------------------------------------------------------------ plan
@@ -243,39 +245,41 @@ __global__ void __launch_bounds__(kThreads) k_stats_exact(TreeLevelArgs a) {
 // ------------------------------------------------------------------ fast stats
 __global__ void __launch_bounds__(kThreads) k_stats_partial(TreeLevelArgs a) {
   __shared__ double sh[2 * kWarps];
-  const int u = blockIdx.x;
-  if (u >= *a.n_units) return;
-  const int g = a.unit_node[u];
-  const int t = g >> a.level;
-  const NodeRange r = node_range(a, g);
-  const int64_t lo = a.unit_lo[u];
-  const int len = (int)min64(kUnit, r.hi - lo);
-  const float *v = tree_vals(a, t) + lo;
-  double s1 = 0.0, s2 = 0.0;
-  for (int i = threadIdx.x; i < len; i += kThreads) {
-    const double x = (double)__ldg(v + i);
-    s1 += x;
-    s2 += x * x;
-  }
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    s1 += __shfl_down_sync(kFull, s1, o);
-    s2 += __shfl_down_sync(kFull, s2, o);
-  }
-  if (lane == 0) {
-    sh[2 * w] = s1;
-    sh[2 * w + 1] = s2;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t1 = 0.0, t2 = 0.0;
-    for (int i = 0; i < kWarps; ++i) {
-      t1 += sh[2 * i];
-      t2 += sh[2 * i + 1];
+  const int n_units = *a.n_units;
+  for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
+    const int g = a.unit_node[u];
+    const int t = g >> a.level;
+    const NodeRange r = node_range(a, g);
+    const int64_t lo = a.unit_lo[u];
+    const int len = (int)min64(kUnit, r.hi - lo);
+    const float *v = tree_vals(a, t) + lo;
+    double s1 = 0.0, s2 = 0.0;
+    for (int i = threadIdx.x; i < len; i += kThreads) {
+      const double x = (double)__ldg(v + i);
+      s1 += x;
+      s2 += x * x;
     }
-    a.unit_s[2 * u] = t1;
-    a.unit_s[2 * u + 1] = t2;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s1 += __shfl_down_sync(kFull, s1, o);
+      s2 += __shfl_down_sync(kFull, s2, o);
+    }
+    if (lane == 0) {
+      sh[2 * w] = s1;
+      sh[2 * w + 1] = s2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t1 = 0.0, t2 = 0.0;
+      for (int i = 0; i < kWarps; ++i) {
+        t1 += sh[2 * i];
+        t2 += sh[2 * i + 1];
+      }
+      a.unit_s[2 * u] = t1;
+      a.unit_s[2 * u + 1] = t2;
+    }
+    __syncthreads();  // sh is reused by the next unit
   }
 }
 
@@ -311,27 +315,29 @@ __global__ void k_bounds_fast(TreeLevelArgs a) {
 __global__ void __launch_bounds__(kThreads) k_hist(TreeLevelArgs a) {
   __shared__ unsigned hist[kWarps][kBins];
   __shared__ float Ds[kBins];
-  const int u = blockIdx.x;
-  if (u >= *a.n_units) return;
-  const int g = a.unit_node[u];
-  const int t = g >> a.level;
-  const NodeRange r = node_range(a, g);
-  const int64_t lo = a.unit_lo[u];
-  const int len = (int)min64(kUnit, r.hi - lo);
-  const float *v = tree_vals(a, t) + lo;
-  if (threadIdx.x < kBins) Ds[threadIdx.x] = a.node_D[(int64_t)g * kBins + threadIdx.x];
-  for (int i = threadIdx.x; i < kWarps * kBins; i += kThreads) (&hist[0][0])[i] = 0u;
-  __syncthreads();
-  float D[kBins];
+  const int n_units = *a.n_units;
+  for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
+    const int g = a.unit_node[u];
+    const int t = g >> a.level;
+    const NodeRange r = node_range(a, g);
+    const int64_t lo = a.unit_lo[u];
+    const int len = (int)min64(kUnit, r.hi - lo);
+    const float *v = tree_vals(a, t) + lo;
+    if (threadIdx.x < kBins) Ds[threadIdx.x] = a.node_D[(int64_t)g * kBins + threadIdx.x];
+    for (int i = threadIdx.x; i < kWarps * kBins; i += kThreads) (&hist[0][0])[i] = 0u;
+    __syncthreads();
+    float D[kBins];
 #pragma unroll
-  for (int j = 0; j < kBins; ++j) D[j] = Ds[j];
-  const int w = threadIdx.x >> 5;
-  for (int i = threadIdx.x; i < len; i += kThreads) atomicAdd(&hist[w][bin_of(D, __ldg(v + i))], 1u);
-  __syncthreads();
-  if (threadIdx.x < kBins) {
-    unsigned tot = 0;
-    for (int k = 0; k < kWarps; ++k) tot += hist[k][threadIdx.x];
-    a.unit_hist[(int64_t)u * kBins + threadIdx.x] = tot;
+    for (int j = 0; j < kBins; ++j) D[j] = Ds[j];
+    const int w = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < len; i += kThreads) atomicAdd(&hist[w][bin_of(D, __ldg(v + i))], 1u);
+    __syncthreads();
+    if (threadIdx.x < kBins) {
+      unsigned tot = 0;
+      for (int k = 0; k < kWarps; ++k) tot += hist[k][threadIdx.x];
+      a.unit_hist[(int64_t)u * kBins + threadIdx.x] = tot;
+    }
+    __syncthreads();  // hist and Ds are reused by the next unit
   }
 }
 
@@ -357,7 +363,13 @@ __global__ void k_median(TreeLevelArgs a) {
   float D[kBins];
 #pragma unroll
   for (int j = 0; j < kBins; ++j) D[j] = a.node_D[(int64_t)g * kBins + j];
-  const float med = node_median(D, h, r.hi - r.lo);
+  float med = node_median(D, h, r.hi - r.lo);
+  if (a.stop) {
+    // root slot s0 of the first level owns the nodes s0 << depth .. below it;
+    // from depth stop[s0] on its nodes keep every point (median +inf)
+    const int nodes = 1 << a.level, depth = a.level - a.p_level0;
+    if (depth >= a.stop[(g & (nodes - 1)) >> depth]) med = __int_as_float(0x7f800000);
+  }
   a.node_med[g] = med;
   if (a.medians) {
     const int nodes = 1 << a.level, t = g >> a.level, s = g & (nodes - 1);
@@ -368,25 +380,27 @@ __global__ void k_median(TreeLevelArgs a) {
 // ------------------------------------------------------------------ count
 __global__ void __launch_bounds__(kThreads) k_count(TreeLevelArgs a) {
   __shared__ int sh[kWarps];
-  const int u = blockIdx.x;
-  if (u >= *a.n_units) return;
-  const int g = a.unit_node[u];
-  const int t = g >> a.level;
-  const NodeRange r = node_range(a, g);
-  const int64_t lo = a.unit_lo[u];
-  const int len = (int)min64(kUnit, r.hi - lo);
-  const float *v = tree_vals(a, t) + lo;
-  const float med = a.node_med[g];
-  int c = 0;
-  for (int i = threadIdx.x; i < len; i += kThreads) c += (__ldg(v + i) <= med) ? 1 : 0;  // :308
+  const int n_units = *a.n_units;
+  for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
+    const int g = a.unit_node[u];
+    const int t = g >> a.level;
+    const NodeRange r = node_range(a, g);
+    const int64_t lo = a.unit_lo[u];
+    const int len = (int)min64(kUnit, r.hi - lo);
+    const float *v = tree_vals(a, t) + lo;
+    const float med = a.node_med[g];
+    int c = 0;
+    for (int i = threadIdx.x; i < len; i += kThreads) c += (__ldg(v + i) <= med) ? 1 : 0;  // :308
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = c;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int tot = 0;
-    for (int k = 0; k < kWarps; ++k) tot += sh[k];
-    a.unit_left[u] = tot;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int tot = 0;
+      for (int k = 0; k < kWarps; ++k) tot += sh[k];
+      a.unit_left[u] = tot;
+    }
+    __syncthreads();  // sh is reused by the next unit
   }
 }
 
@@ -425,67 +439,70 @@ __global__ void __launch_bounds__(kThreads) k_scatter(TreeLevelArgs a) {
   __shared__ int32_t sid[kUnit];
   __shared__ float sval[kUnit];
   __shared__ int wsum[kWarps];
-  const int u = blockIdx.x;
-  if (u >= *a.n_units) return;
-  const int g = a.unit_node[u];
-  const int t = g >> a.level;
-  const NodeRange r = node_range(a, g);
-  const int64_t lo = a.unit_lo[u];
-  const int len = (int)min64(kUnit, r.hi - lo);
-  const float *v = tree_vals(a, t) + lo;
-  const float med = a.node_med[g];
-  // each thread owns kPer consecutive positions
-  const int p0 = threadIdx.x * kPer;
-  unsigned mask = 0;
-  int my = 0;
+  const int n_units = *a.n_units;
+  for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
+    const int g = a.unit_node[u];
+    const int t = g >> a.level;
+    const NodeRange r = node_range(a, g);
+    const int64_t lo = a.unit_lo[u];
+    const int len = (int)min64(kUnit, r.hi - lo);
+    const float *v = tree_vals(a, t) + lo;
+    const float med = a.node_med[g];
+    // each thread owns kPer consecutive positions
+    const int p0 = threadIdx.x * kPer;
+    unsigned mask = 0;
+    int my = 0;
 #pragma unroll
-  for (int j = 0; j < kPer; ++j) {
-    const int p = p0 + j;
-    if (p < len && __ldg(v + p) <= med) {
-      mask |= 1u << j;
-      ++my;
+    for (int j = 0; j < kPer; ++j) {
+      const int p = p0 + j;
+      if (p < len && __ldg(v + p) <= med) {
+        mask |= 1u << j;
+        ++my;
+      }
     }
-  }
-  // exclusive scan of the per-thread left counts
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int x = my;
+    // exclusive scan of the per-thread left counts
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = my;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(kFull, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) wsum[w] = x;
-  __syncthreads();
-  int wbase = 0, ltot = 0;
-  for (int k = 0; k < kWarps; ++k) {
-    if (k < w) wbase += wsum[k];
-    ltot += wsum[k];
-  }
-  int lrank = wbase + x - my;            // left-goers before p0 in the unit
-  int rrank = ltot + (p0 - lrank);       // slot of this thread's first right-goer
-  const int32_t *oin = a.ord_in ? a.ord_in + (int64_t)t * a.n + lo : nullptr;
-  const bool want_val = a.val_out != nullptr;
-  const float *pnext = want_val ? a.P + ((int64_t)t * (a.gd - 1) + a.level + 1) * a.n : nullptr;
-#pragma unroll
-  for (int j = 0; j < kPer; ++j) {
-    const int p = p0 + j;
-    if (p < len) {
-      const int32_t id = oin ? __ldg(oin + p) : (int32_t)(lo + p);
-      const int slot = ((mask >> j) & 1u) ? lrank++ : rrank++;
-      sid[slot] = id;
-      if (want_val) sval[slot] = __ldg(pnext + id);
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, x, o);
+      if (lane >= o) x += y;
     }
-  }
-  __syncthreads();
-  // left-goers -> [node lo + unit lbase, ...), right-goers -> [node lo + nleft + rbase, ...)
-  const int64_t lbase = r.lo + a.unit_lbase[u];
-  const int64_t rbase = r.lo + a.node_nleft[g] + (lo - r.lo - a.unit_lbase[u]);
-  int32_t *oout = a.ord_out + (int64_t)t * a.n;
-  float *vout = want_val ? a.val_out + (int64_t)t * a.n : nullptr;
-  for (int i = threadIdx.x; i < len; i += kThreads) {
-    const int64_t dst = i < ltot ? lbase + i : rbase + (i - ltot);
-    oout[dst] = sid[i];
-    if (want_val) vout[dst] = sval[i];
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    int wbase = 0, ltot = 0;
+    for (int k = 0; k < kWarps; ++k) {
+      if (k < w) wbase += wsum[k];
+      ltot += wsum[k];
+    }
+    int lrank = wbase + x - my;            // left-goers before p0 in the unit
+    int rrank = ltot + (p0 - lrank);       // slot of this thread's first right-goer
+    const int32_t *oin = a.ord_in ? a.ord_in + (int64_t)t * a.n + lo : nullptr;
+    const bool want_val = a.val_out != nullptr;
+    const float *pnext =
+        want_val ? a.P + ((int64_t)t * (a.gd - 1) + a.level - a.p_level0 + 1) * a.n : nullptr;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      const int p = p0 + j;
+      if (p < len) {
+        const int32_t id = oin ? __ldg(oin + p) : (int32_t)(lo + p);
+        const int slot = ((mask >> j) & 1u) ? lrank++ : rrank++;
+        sid[slot] = id;
+        if (want_val) sval[slot] = __ldg(pnext + id);
+      }
+    }
+    __syncthreads();
+    // left-goers -> [node lo + unit lbase, ...), right-goers -> [node lo + nleft + rbase, ...)
+    const int64_t lbase = r.lo + a.unit_lbase[u];
+    const int64_t rbase = r.lo + a.node_nleft[g] + (lo - r.lo - a.unit_lbase[u]);
+    int32_t *oout = a.ord_out + (int64_t)t * a.n;
+    float *vout = want_val ? a.val_out + (int64_t)t * a.n : nullptr;
+    for (int i = threadIdx.x; i < len; i += kThreads) {
+      const int64_t dst = i < ltot ? lbase + i : rbase + (i - ltot);
+      oout[dst] = sid[i];
+      if (want_val) vout[dst] = sval[i];
+    }
+    __syncthreads();  // sid, sval and wsum are reused by the next unit
   }
 }
 
@@ -497,7 +514,9 @@ drpt_status launch_tree_level(const TreeLevelArgs &a, int64_t max_units, cudaStr
     set_error("too many tree nodes at level %d", a.level);
     return DRPT_ERR_UNSUPPORTED;
   }
-  const unsigned U = (unsigned)max_units, gn = (unsigned)ceil_div(G * 32, 256);  // warp per node
+  // unit kernels loop over the units actually planned (grid-stride)
+  const unsigned U = (unsigned)min64(max_units, 148 * 16);
+  const unsigned gn = (unsigned)ceil_div(G * 32, 256);  // warp per node
   k_plan<<<1, 1024, 0, s>>>(a);
   if (a.exact) {
     k_stats_exact<<<(unsigned)G, kThreads, 0, s>>>(a);

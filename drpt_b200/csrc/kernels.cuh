@@ -11,11 +11,17 @@ namespace drpt {
 // Column c of P (column-major, ncols x n) is sum over the nonzeros (k, b) of
 // B's column, in ascending k, of x[k] * b with one rounding per operation.
 struct CscDev {
-  const int32_t *colptr;  // ncols + 1
+  const int32_t *colptr;  // ncols + 1 (x column sets with a block table)
   const int32_t *row;     // nnz, ascending within a column
   const float *val;       // nnz
   int32_t ncols;
+  // Optional block table (batches): nblocks entries {first point, points
+  // (<= project_points_per_block), column set}; column set c uses colptr
+  // entries [c * (ncols + 1), (c + 1) * (ncols + 1)).
+  const int32_t *blocks = nullptr;
+  int32_t nblocks = 0;
 };
+int project_points_per_block(int d);
 drpt_status launch_project(const void *X, int dtype, int64_t n, int d, const CscDev &csc,
                            float *P, cudaStream_t s);
 
@@ -32,6 +38,9 @@ struct TreeLevelArgs {
   int32_t *off_out;        // T x (2^(level+1) + 1)
   float *medians;          // T x (2^(gd-1) - 1) heap order, or nullptr
   int exact;               // sequential FP32 statistics
+  int p_level0;            // level that reads P directly (0; a batch's root level)
+  const int8_t *stop;      // batches: per root slot of level p_level0, the depth
+                           // from which its nodes keep all points; nullptr = none
   // scratch (G = T * 2^level nodes, U = tree_level_max_units units)
   int32_t *node_ubase;     // G + 1
   int32_t *unit_node;      // U
@@ -103,6 +112,10 @@ struct MixedTreeArgs {
   int *err;                  // set when a bounded wait gave up
 };
 int mixed_d_pad(int d, int fp8);
+// Batches: ids of point p's neighbours made relative to its dataset's first
+// row (set_off: nsets + 1 row offsets, device).
+drpt_status launch_localize(int32_t *idx, int64_t n, int k, const int64_t *set_off, int nsets,
+                            cudaStream_t s);
 drpt_status launch_leaf_center(const MixedTreeArgs &a, cudaStream_t s);
 drpt_status launch_leaf_mma(const MixedTreeArgs &a, cudaStream_t s);
 drpt_status launch_rerank(const void *X, int dtype, int d, const int32_t *visit, int64_t n,

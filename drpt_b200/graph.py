@@ -20,7 +20,8 @@ import numpy as np
 from . import _lib
 from ._lib import DrptError, Stats, check
 
-__all__ = ["build_graph", "MDRPT", "DrptError", "edge_list_lines", "global_depth"]
+__all__ = ["build_graph", "build_graph_batched", "MDRPT", "DrptError", "edge_list_lines",
+           "global_depth"]
 
 
 def _torch():
@@ -113,6 +114,58 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
     stats = Stats()
     check(_lib.load().drpt_build_graph(ctx.handle, ctypes.byref(desc), ptr_data, ptr_idx, ptr_dist,
                                        ctypes.byref(stats)))
+    return idx, dist, stats
+
+
+def build_graph_batched(data, offsets, ntrees: int, nn: int, seed: int, *, mode: str = "mixed",
+                        leaf_size: int = 0, precision: str = "bf16", density: float = 0.0,
+                        use_graph: bool = False, stream=None, out=None):
+    """k-NN graphs of many independent datasets in one call
+    (drpt_build_graph_batched).  `data` holds the datasets row after row (a
+    NumPy array or a CUDA tensor, uint8 or float32); dataset s is rows
+    offsets[s]:offsets[s+1].  Returns (idx, dist, stats) with idx relative to
+    each dataset's first row; each dataset's rows equal build_graph on that
+    dataset alone.  `use_graph` captures the device work in a CUDA graph and
+    replays it on later calls with the same offsets, parameters and tensors
+    (CUDA tensors only)."""
+    offs = np.ascontiguousarray(np.asarray(offsets, dtype=np.int64))
+    on_dev = _is_cuda_tensor(data)
+    data = data.contiguous() if on_dev else np.ascontiguousarray(data)
+    n, d = int(data.shape[0]), int(data.shape[1])
+    if offs[-1] != n:
+        raise DrptError(1, f"offsets end at {offs[-1]}, data has {n} rows")
+    desc = _lib.BatchDesc()
+    desc.nsets, desc.d, desc.dtype = len(offs) - 1, d, _dtype_code(data)
+    desc.ntrees, desc.nn = ntrees, nn
+    desc.mode = {"mixed": _lib.MODE_MIXED, "fp32_leaf": _lib.MODE_FP32_LEAF}[mode]
+    desc.precision = {"bf16": _lib.PRECISION_BF16, "fp8": _lib.PRECISION_FP8_E4M3}[precision]
+    desc.leaf_size, desc.seed, desc.density = leaf_size, seed & 0xFFFFFFFF, density
+    desc.use_graph = 1 if use_graph else 0
+    desc.data_on_device = desc.out_on_device = 1 if on_dev else 0
+    if on_dev:
+        torch = _torch()
+        if stream is None:
+            stream = torch.cuda.current_stream(data.device).cuda_stream
+        device = data.device.index if data.device.index is not None else 0
+        if out is None:
+            idx = torch.empty((n, nn), dtype=torch.int32, device=data.device)
+            dist = torch.empty((n, nn), dtype=torch.float32, device=data.device)
+        else:
+            idx, dist = out
+        ptrs = (data.data_ptr(), idx.data_ptr(), dist.data_ptr())
+    else:
+        device = 0
+        if out is None:
+            idx = np.empty((n, nn), np.int32)
+            dist = np.empty((n, nn), np.float32)
+        else:
+            idx, dist = out
+        ptrs = (data.ctypes.data, idx.ctypes.data, dist.ctypes.data)
+    desc.stream = stream or 0
+    ctx = _lib.context(device)
+    stats = Stats()
+    check(_lib.load().drpt_build_graph_batched(ctx.handle, ctypes.byref(desc), offs.ctypes.data,
+                                               ptrs[0], ptrs[1], ptrs[2], ctypes.byref(stats)))
     return idx, dist, stats
 
 

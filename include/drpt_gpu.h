@@ -147,6 +147,42 @@ void drpt_ctx_destroy(drpt_ctx *ctx);
 drpt_status drpt_build_graph(drpt_ctx *ctx, const drpt_build_desc *desc, const void *data,
                              int32_t *out_idx, float *out_dist, drpt_stats *stats);
 
+/* A batch of independent k-NN-graph builds (no reference counterpart: the
+ * reference builds one dataset per process run).  The datasets share d,
+ * dtype and the build parameters and lie row-wise one after another in
+ * `data`; dataset s is rows [offsets[s], offsets[s+1]). */
+typedef struct {
+  int32_t nsets;              /* datasets in the batch (1 .. 65536) */
+  int32_t d;                  /* dimensions of every dataset */
+  int32_t dtype;              /* drpt_dtype */
+  int32_t ntrees;
+  int32_t nn;
+  int32_t mode;               /* DRPT_MODE_MIXED or DRPT_MODE_FP32_LEAF */
+  int32_t precision;          /* drpt_precision (mixed mode) */
+  int32_t leaf_size;          /* target global leaf size (0 = 512) */
+  uint32_t seed;              /* projection seed, the same for every dataset */
+  int32_t use_graph;          /* 1: capture the device work of this batch in a
+                                 CUDA graph and replay it on later calls with
+                                 the same offsets, parameters and pointers
+                                 (device pointers only) */
+  double density;             /* 0: 1/sqrt(d) */
+  int32_t data_on_device;     /* 1: data is device memory */
+  int32_t out_on_device;      /* 1: outputs are device memory */
+  void *stream;               /* cudaStream_t; NULL = legacy default */
+} drpt_batch_desc;
+
+/* Builds every dataset of the batch together: one projection launch, one
+ * launch per kernel and tree level, one leaf-kernel launch per tree and one
+ * re-rank launch over all datasets.  Each dataset's graph equals
+ * drpt_build_graph's for that dataset alone with the same parameters.
+ * `offsets` is a host array of nsets + 1 row offsets (offsets[0] = 0,
+ * non-decreasing, every dataset at least 2 rows).  out_idx / out_dist
+ * (total rows x nn) hold neighbour ids relative to their dataset's first
+ * row. */
+drpt_status drpt_build_graph_batched(drpt_ctx *ctx, const drpt_batch_desc *desc,
+                                     const int64_t *offsets, const void *data, int32_t *out_idx,
+                                     float *out_dist, drpt_stats *stats);
+
 /* The reference's sparse Gaussian projection matrix on the host, d x L
  * row-major, from std::mt19937(seed) (math_operations.cpp:48-76). */
 drpt_status drpt_host_projection(uint32_t seed, int32_t d, int32_t L, float density, float *B);
