@@ -27,7 +27,7 @@ EXPORTS = [
     "drpt_version", "drpt_last_error", "drpt_ctx_create", "drpt_ctx_destroy", "drpt_build_graph",
     "drpt_host_projection", "drpt_project", "drpt_global_trees", "drpt_local_leaves",
     "drpt_leaf_knn", "drpt_merge_candidates", "drpt_global_trees_noalloc",
-    "drpt_build_graph_batched",
+    "drpt_build_graph_batched", "drpt_learn_gradient",
 ]
 
 
@@ -49,6 +49,8 @@ class BuildDesc(ctypes.Structure):
         ("local_seeds", ctypes.POINTER(ctypes.c_uint32)), ("mode", ctypes.c_int32),
         ("data_on_device", ctypes.c_int32), ("out_on_device", ctypes.c_int32),
         ("stream", ctypes.c_void_p), ("leaf_size", ctypes.c_int32), ("precision", ctypes.c_int32),
+        ("learned_trees", ctypes.c_int32), ("learn_sample", ctypes.c_int32),
+        ("learn_iters", ctypes.c_int32), ("reserved", ctypes.c_int32),
     ]
 
 
@@ -74,10 +76,13 @@ class Stats(ctypes.Structure):
         ("ms_leaf_knn", ctypes.c_float), ("ms_merge", ctypes.c_float), ("ms_total", ctypes.c_float),
         ("ms_leaf_mma", ctypes.c_float), ("ms_leaf_stage", ctypes.c_float),
         ("mma_pairs_padded", ctypes.c_int64),
+        ("ms_learn", ctypes.c_float), ("learn_loss_start", ctypes.c_float),
+        ("learn_loss_end", ctypes.c_float), ("reserved2", ctypes.c_int32),
     ]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+        return {name: getattr(self, name) for name, _ in self._fields_
+                if not name.startswith("reserved")}
 
 
 _lib = None
@@ -110,6 +115,7 @@ def load(path: str = LIB_PATH):
         L.drpt_leaf_knn.argtypes = [vp, vp, i32, i64, i32, i32, vp, vp, i32, i32, vp, vp, vp]
         L.drpt_merge_candidates.argtypes = [vp, vp, vp, i64, i32, i32, vp, vp, vp]
         L.drpt_global_trees_noalloc.argtypes = [vp, i64, i32, i32, i32, vp, vp, vp, vp]
+        L.drpt_learn_gradient.argtypes = [vp, vp, i32, i32, vp, vp, vp, i32, vp, vp]
         L.drpt_build_graph_batched.argtypes = [vp, ctypes.POINTER(BatchDesc), vp, vp, vp, vp,
                                                ctypes.POINTER(Stats)]
         for name in EXPORTS:

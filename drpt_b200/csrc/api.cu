@@ -17,6 +17,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <random>
 #include <string>
 #include <utility>
 #include <vector>
@@ -421,6 +422,259 @@ drpt_status mixed_check(drpt_ctx *c, cudaStream_t s) {
   return DRPT_OK;
 }
 
+// ---------------------------------------------------------------- learned splits
+// Per learned tree and level an MLP d -> 64 -> 1 (k_learned.cu).  Training
+// runs level by level on a sample: the sample's 10 nearest neighbours come
+// from the mixed form's own leaf brute force (the whole sample as one leaf),
+// each level's MLPs of all learned trees train together with Adam, and the
+// sample is then split by the level kernels on the trained outputs (the
+// histogram median of every node, as the full trees split) to give the next
+// level's nodes.  Inference writes every MLP's output for all n points into
+// the projected-column array P, where the level kernels split on it exactly
+// as on a random projection.
+constexpr int kLearnIters = 10;      // default Adam steps per level
+constexpr int kLearnSample = 8192;   // default sample size
+constexpr float kLearnLr = 0.01f;
+constexpr int kLearnPairs = 10;      // neighbours per sample point
+constexpr int kLearnChunks = 64;     // row chunks of the backward pass
+
+// Reverse neighbour pairs (CSR over the S sample points), each row ascending.
+void pair_tables(const std::vector<int32_t> &nbr, int S, int k, std::vector<int32_t> *in_ptr,
+                 std::vector<int32_t> *in_idx) {
+  in_ptr->assign(S + 1, 0);
+  for (int i = 0; i < S; ++i)
+    for (int q = 0; q < k; ++q) {
+      const int j = nbr[(size_t)i * k + q];
+      if (j >= 0) ++(*in_ptr)[j + 1];
+    }
+  for (int i = 0; i < S; ++i) (*in_ptr)[i + 1] += (*in_ptr)[i];
+  in_idx->assign((*in_ptr)[S], 0);
+  std::vector<int32_t> fill(in_ptr->begin(), in_ptr->end() - 1);
+  for (int i = 0; i < S; ++i)
+    for (int q = 0; q < k; ++q) {
+      const int j = nbr[(size_t)i * k + q];
+      if (j >= 0) (*in_idx)[fill[j]++] = i;
+    }
+}
+
+// Device buffers of a training run: T trees, S sample points, node tables for
+// up to max_nodes nodes per tree.
+drpt_status learn_buffers(drpt_ctx *c, int T, int S, int d, int k, int max_nodes, LearnArgs *a) {
+  a->S = S;
+  a->d = d;
+  a->T = T;
+  a->k = k;
+  a->np = kLearnHidden * d + 2 * kLearnHidden + 1;
+  a->R = kLearnChunks;
+  const size_t ts = (size_t)T * S, tp = (size_t)T * a->np, tn = (size_t)T * max_nodes;
+  float *Xs, *inv;
+  int32_t *nbr, *in_ptr, *in_idx;
+  DRPT_TRY(ws_get(c, "ln_xs", (size_t)S * d, &Xs));
+  DRPT_TRY(ws_get(c, "ln_params", tp, &a->params));
+  DRPT_TRY(ws_get(c, "ln_m1", tp, &a->m1));
+  DRPT_TRY(ws_get(c, "ln_m2", tp, &a->m2));
+  DRPT_TRY(ws_get(c, "ln_nbr", (size_t)S * k, &nbr));
+  DRPT_TRY(ws_get(c, "ln_in_ptr", (size_t)S + 1, &in_ptr));
+  DRPT_TRY(ws_get(c, "ln_in_idx", (size_t)S * k, &in_idx));
+  DRPT_TRY(ws_get(c, "ln_inv_pairs", (size_t)T, &inv));
+  DRPT_TRY(ws_get(c, "ln_A", ts * kLearnHidden, &a->A));
+  DRPT_TRY(ws_get(c, "ln_f", ts, &a->f));
+  DRPT_TRY(ws_get(c, "ln_g", ts, &a->g));
+  DRPT_TRY(ws_get(c, "ln_sp", ts, &a->sp));
+  DRPT_TRY(ws_get(c, "ln_mu", tn, &a->mu));
+  DRPT_TRY(ws_get(c, "ln_var", tn, &a->var));
+  DRPT_TRY(ws_get(c, "ln_sn", tn, &a->sn));
+  DRPT_TRY(ws_get(c, "ln_lterm", tn, &a->lterm));
+  DRPT_TRY(ws_get(c, "ln_part", (size_t)T * a->R * a->np, &a->part));
+  a->Xs = Xs;
+  a->nbr = nbr;
+  a->in_ptr = in_ptr;
+  a->in_idx = in_idx;
+  a->inv_pairs = inv;
+  return DRPT_OK;
+}
+
+struct LearnResult {
+  float loss_start = 0.0f, loss_end = 0.0f;
+};
+
+// Trains the split MLPs of T learned trees of global depth gd and writes
+// their outputs for all n points to P columns [col0, col0 + T*(gd-1)).
+drpt_status learn_and_project(drpt_ctx *c, const void *X, int dtype, int64_t n, int d, int T,
+                              int gd, uint32_t seed, int sample, int iters, float *P,
+                              int64_t col0, LearnResult *res, cudaStream_t s) {
+  const int levels = gd - 1;
+  if (levels <= 0) return DRPT_OK;
+  const int S = (int)std::min<int64_t>(n, sample > 0 ? sample : kLearnSample);
+  if (iters <= 0) iters = kLearnIters;
+  const int d_pad = (d + 63) / 64 * 64;
+  // sample rows: S distinct indices, ascending
+  std::mt19937 gen(seed ^ 0x5bd1e995u);
+  std::vector<int32_t> ids(n);
+  for (int64_t i = 0; i < n; ++i) ids[i] = (int32_t)i;
+  for (int i = 0; i < S; ++i) {
+    std::uniform_int_distribution<int64_t> pick(i, n - 1);
+    std::swap(ids[i], ids[pick(gen)]);
+  }
+  ids.resize(S);
+  std::sort(ids.begin(), ids.end());
+  int32_t *dids;
+  float *xraw, *dc, *dinv;
+  double *dvar;
+  DRPT_TRY(ws_get(c, "ln_ids", (size_t)S, &dids));
+  DRPT_TRY(ws_get(c, "ln_xraw", (size_t)S * d, &xraw));
+  DRPT_TRY(ws_get(c, "ln_c", (size_t)d, &dc));
+  DRPT_TRY(ws_get(c, "ln_dvar", (size_t)d, &dvar));
+  DRPT_TRY(ws_get(c, "ln_inv_sigma", 1, &dinv));
+  DRPT_CUDA(cudaMemcpyAsync(dids, ids.data(), (size_t)S * 4, cudaMemcpyHostToDevice, s));
+  DRPT_TRY(launch_standardise(X, dtype, S, d, d, dids, nullptr, nullptr, nullptr, xraw, s));
+  DRPT_TRY(launch_sample_scale(xraw, S, d, dc, dvar, dinv, s));
+  // the sample's neighbours: the mixed leaf brute force over one leaf
+  int32_t *iota_t, *goff1, *nbr_d;
+  float *ndist;
+  const int max_nodes = 1 << (levels - 1);
+  DRPT_TRY(ws_get(c, "ln_iota", (size_t)T * S, &iota_t));
+  DRPT_TRY(ws_get(c, "ln_goff", (size_t)2 * T, &goff1));
+  DRPT_TRY(ws_get(c, "ln_knn_idx", (size_t)S * kLearnPairs, &nbr_d));
+  DRPT_TRY(ws_get(c, "ln_knn_dist", (size_t)S * kLearnPairs, &ndist));
+  std::vector<int32_t> io((size_t)T * S), g2(2 * T);
+  for (int t = 0; t < T; ++t) {
+    for (int i = 0; i < S; ++i) io[(size_t)t * S + i] = i;
+    g2[2 * t] = 0;
+    g2[2 * t + 1] = S;
+  }
+  DRPT_CUDA(cudaMemcpyAsync(iota_t, io.data(), io.size() * 4, cudaMemcpyHostToDevice, s));
+  DRPT_CUDA(cudaMemcpyAsync(goff1, g2.data(), g2.size() * 4, cudaMemcpyHostToDevice, s));
+  DRPT_TRY(mixed_leaf_phase(c, xraw, DRPT_DTYPE_F32, S, d, 1, kLearnPairs, 0, iota_t, goff1, 1,
+                            nbr_d, ndist, false, s));
+  DRPT_TRY(mixed_check(c, s));
+  std::vector<int32_t> nbr((size_t)S * kLearnPairs);
+  DRPT_CUDA(cudaMemcpy(nbr.data(), nbr_d, nbr.size() * 4, cudaMemcpyDeviceToHost));
+  // training state
+  LearnArgs a{};
+  DRPT_TRY(learn_buffers(c, T, S, d, kLearnPairs, max_nodes, &a));
+  DRPT_TRY(launch_standardise(X, dtype, S, d, d, dids, dc, dinv, nullptr, (float *)a.Xs, s));
+  DRPT_CUDA(cudaMemcpyAsync((void *)a.nbr, nbr.data(), nbr.size() * 4, cudaMemcpyHostToDevice, s));
+  std::vector<int32_t> in_ptr, in_idx;
+  pair_tables(nbr, S, kLearnPairs, &in_ptr, &in_idx);
+  DRPT_CUDA(cudaMemcpyAsync((void *)a.in_ptr, in_ptr.data(), in_ptr.size() * 4,
+                            cudaMemcpyHostToDevice, s));
+  if (!in_idx.empty())
+    DRPT_CUDA(cudaMemcpyAsync((void *)a.in_idx, in_idx.data(), in_idx.size() * 4,
+                              cudaMemcpyHostToDevice, s));
+  // node tables, ping-pong: level 0 is one node per tree holding the sample
+  int32_t *perm[2], *noff[2], *node_of, *cnt;
+  float *fp, *loss;
+  DRPT_TRY(ws_get(c, "ln_perm_a", (size_t)T * S, &perm[0]));
+  DRPT_TRY(ws_get(c, "ln_perm_b", (size_t)T * S, &perm[1]));
+  DRPT_TRY(ws_get(c, "ln_noff_a", (size_t)T * (2 * max_nodes + 1), &noff[0]));
+  DRPT_TRY(ws_get(c, "ln_noff_b", (size_t)T * (2 * max_nodes + 1), &noff[1]));
+  DRPT_TRY(ws_get(c, "ln_node_of", (size_t)T * S, &node_of));
+  DRPT_TRY(ws_get(c, "ln_cnt", (size_t)T, &cnt));
+  DRPT_TRY(ws_get(c, "ln_fp", (size_t)T * S, &fp));
+  DRPT_TRY(ws_get(c, "ln_loss", 2, &loss));
+  DRPT_CUDA(cudaMemcpyAsync(perm[0], iota_t, (size_t)T * S * 4, cudaMemcpyDeviceToDevice, s));
+  DRPT_CUDA(cudaMemcpyAsync(noff[0], goff1, (size_t)2 * T * 4, cudaMemcpyDeviceToDevice, s));
+  DRPT_CUDA(cudaMemsetAsync(node_of, 0, (size_t)T * S * 4, s));
+  DRPT_CUDA(cudaMemsetAsync(loss, 0, 2 * sizeof(float), s));
+  // level-kernel scratch for the sample splits (deepest split level: levels - 2)
+  TreeLevelArgs lv{};
+  if (levels >= 2) {
+    const int last = levels - 2;
+    const int64_t Gmax = (int64_t)T << last, Umax = tree_level_max_units(S, T, last);
+    DRPT_TRY(ws_get(c, "ls_node_ubase", Gmax + 1, &lv.node_ubase));
+    DRPT_TRY(ws_get(c, "ls_unit_node", Umax, &lv.unit_node));
+    DRPT_TRY(ws_get(c, "ls_unit_lo", Umax, &lv.unit_lo));
+    DRPT_TRY(ws_get(c, "ls_n_units", 1, &lv.n_units));
+    DRPT_TRY(ws_get(c, "ls_node_D", Gmax * kBins, &lv.node_D));
+    DRPT_TRY(ws_get(c, "ls_unit_s", 2 * Umax, &lv.unit_s));
+    DRPT_TRY(ws_get(c, "ls_unit_hist", Umax * kBins, &lv.unit_hist));
+    DRPT_TRY(ws_get(c, "ls_node_med", Gmax, &lv.node_med));
+    DRPT_TRY(ws_get(c, "ls_unit_left", Umax, &lv.unit_left));
+    DRPT_TRY(ws_get(c, "ls_unit_lbase", Umax, &lv.unit_lbase));
+    DRPT_TRY(ws_get(c, "ls_node_nleft", Gmax, &lv.node_nleft));
+  }
+  // stacked inference weights, MLP m = tree * levels + level
+  const int M = T * levels;
+  __nv_bfloat16 *wb;
+  float *db1, *dw2, *db2;
+  DRPT_TRY(ws_get(c, "ln_w1b", (size_t)M * kLearnHidden * d_pad, &wb));
+  DRPT_TRY(ws_get(c, "ln_b1", (size_t)M * kLearnHidden, &db1));
+  DRPT_TRY(ws_get(c, "ln_w2", (size_t)M * kLearnHidden, &dw2));
+  DRPT_TRY(ws_get(c, "ln_b2", (size_t)M, &db2));
+  DRPT_CUDA(cudaMemsetAsync(wb, 0, (size_t)M * kLearnHidden * d_pad * 2, s));
+  int cur = 0;
+  for (int l = 0; l < levels; ++l) {
+    const int nodes = 1 << l;
+    a.perm = perm[cur];
+    a.noff = noff[cur];
+    a.node_of = node_of;
+    a.nodes = nodes;
+    DRPT_TRY(launch_learn_pairs(a, cnt, s));
+    DRPT_TRY(launch_learn_init(a, seed, l, s));
+    DRPT_CUDA(cudaMemsetAsync(a.m1, 0, (size_t)T * a.np * 4, s));
+    DRPT_CUDA(cudaMemsetAsync(a.m2, 0, (size_t)T * a.np * 4, s));
+    c->launches += 3;
+    for (int it = 0; it < iters; ++it) {
+      const float bc1 = 1.0f - std::pow(0.9f, (float)(it + 1));
+      const float bc2 = 1.0f - std::pow(0.999f, (float)(it + 1));
+      DRPT_TRY(launch_learn_step(a, kLearnLr, bc1, bc2, nullptr, s));
+      c->launches += learn_step_kernels();
+      if (it == 0) DRPT_TRY(launch_learn_loss(a, loss, 0, s));
+    }
+    // the loss and outputs at the trained weights
+    DRPT_TRY(launch_learn_step(a, 0.0f, 1.0f, 1.0f, nullptr, s));
+    DRPT_TRY(launch_learn_loss(a, loss, 1, s));
+    DRPT_TRY(launch_stack(a, d_pad, levels, l, wb, db1, dw2, db2, s));
+    c->launches += learn_step_kernels() + 3;
+    if (l + 1 < levels) {
+      // split every node of the sample at the histogram median of f
+      DRPT_TRY(launch_gather_f(a, fp, s));
+      TreeLevelArgs t = lv;
+      t.P = nullptr;
+      t.n = S;
+      t.T = T;
+      t.gd = 2;
+      t.level = l;
+      t.p_level0 = -1;  // values come from val_in (f in node order)
+      t.ord_in = perm[cur];
+      t.val_in = fp;
+      t.off_in = noff[cur];
+      t.ord_out = perm[cur ^ 1];
+      t.val_out = nullptr;
+      t.off_out = noff[cur ^ 1];
+      t.medians = nullptr;
+      t.exact = 0;
+      t.stop = nullptr;
+      DRPT_TRY(launch_tree_level(t, tree_level_max_units(S, T, l), s));
+      DRPT_TRY(launch_node_label(perm[cur ^ 1], noff[cur ^ 1], 2 * nodes, S, T, node_of, s));
+      c->launches += tree_level_kernels(0) + 2;
+      cur ^= 1;
+    }
+  }
+  // inference over all n points
+  __nv_bfloat16 *xb;
+  int *err;
+  DRPT_TRY(ws_get(c, "ln_xb", (size_t)n * d_pad, &xb));
+  DRPT_TRY(ws_get(c, "ln_err", 1, &err));
+  DRPT_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  DRPT_TRY(launch_standardise(X, dtype, n, d, d_pad, nullptr, dc, dinv, xb, nullptr, s));
+  DRPT_TRY(launch_mlp_infer(xb, n, d_pad, wb, M, db1, dw2, db2, P + col0 * n, err, s));
+  c->launches += 2;
+  float hl[2] = {0.0f, 0.0f};
+  int herr = 0;
+  DRPT_CUDA(cudaMemcpyAsync(hl, loss, sizeof(hl), cudaMemcpyDeviceToHost, s));
+  DRPT_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DRPT_CUDA(cudaStreamSynchronize(s));
+  if (herr) {
+    set_error("a bounded wait in the split-MLP inference kernel gave up");
+    return DRPT_ERR_TIMEOUT;
+  }
+  res->loss_start = hl[0] / ((float)T * levels);
+  res->loss_end = hl[1] / ((float)T * levels);
+  return DRPT_OK;
+}
+
 // Mixed-precision pipeline (DRPT_MODE_MIXED): global trees with fast
 // statistics grown to leaves of about `leaf_size` points, BF16 tensor-core
 // brute force of every global leaf, cross-tree merge of the approximate
@@ -442,23 +696,44 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
     set_error("mixed mode supports d %% 4 == 0 and d <= 1024 (got %d)", d);
     return DRPT_ERR_UNSUPPORTED;
   }
+  const int learned = desc->learned_trees;
+  if (learned < 0 || learned > T || desc->learn_sample < 0 || desc->learn_iters < 0) {
+    set_error("learned_trees %d (of %d), learn_sample %d or learn_iters %d out of range", learned,
+              T, desc->learn_sample, desc->learn_iters);
+    return DRPT_ERR_INVALID_ARG;
+  }
+  if (learned > 0 && d > 256) {
+    set_error("learned splits support d <= 256 (got %d)", d);
+    return DRPT_ERR_UNSUPPORTED;
+  }
   int gd = 0;
   DRPT_TRY(leaf_depth(n, desc->leaf_size, &gd));
   const int nleaf = 1 << (gd - 1);
-  const int L = gd * T;
+  const int L = gd * T, Tr = T - learned;
   const float density = (float)(desc->density == 0 ? 1.0 / std::sqrt((double)d) : desc->density);
   cudaEvent_t *ev = c->ev;
   const int launches0 = c->launches;
   DRPT_CUDA(cudaEventRecord(ev[1], s));
 
+  // trees 0 .. Tr-1 split on random projections, the learned ones on MLP values
   std::vector<float> B((size_t)d * L);
   host_projection_matrix(desc->seed, d, L, density, B.data());
   std::vector<int32_t> cols;
-  for (int t = 0; t < T; ++t)
+  for (int t = 0; t < Tr; ++t)
     for (int l = 0; l + 1 < gd; ++l) cols.push_back(t * gd + l);
   float *P = nullptr;
-  DRPT_TRY(ws_get(c, "P", std::max<size_t>(cols.size(), 1) * n, &P));
+  DRPT_TRY(ws_get(c, "P", std::max<size_t>((size_t)T * (gd - 1), 1) * n, &P));
   if (!cols.empty()) DRPT_TRY(project_cols(c, X, desc->dtype, n, d, B.data(), L, cols, P, s));
+  LearnResult lres;
+  float ms_learn = 0.0f;
+  if (learned > 0) {
+    const auto t0 = std::chrono::steady_clock::now();
+    DRPT_TRY(learn_and_project(c, X, desc->dtype, n, d, learned, gd, desc->seed,
+                               desc->learn_sample, desc->learn_iters, P, (int64_t)Tr * (gd - 1),
+                               &lres, s));
+    ms_learn =
+        std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
   int32_t *order, *goff;
   DRPT_TRY(global_trees(c, P, n, T, gd, 0, nullptr, &order, &goff, s));
   DRPT_CUDA(cudaEventRecord(ev[2], s));
@@ -505,6 +780,9 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
     stats->ms_local = elapsed(ev[2], ev[3]);
     stats->ms_leaf_knn = elapsed(ev[3], ev[4]);
     stats->ms_merge = elapsed(ev[4], ev[5]);
+    stats->ms_learn = ms_learn;
+    stats->learn_loss_start = lres.loss_start;
+    stats->learn_loss_end = lres.loss_end;
   }
   return DRPT_OK;
 }
@@ -999,6 +1277,58 @@ drpt_status drpt_build_graph_batched(drpt_ctx *c, const drpt_batch_desc *desc,
     c->glaunches = c->launches - l0;
     c->launches = l0;
   }
+  return DRPT_OK;
+}
+
+drpt_status drpt_learn_gradient(drpt_ctx *c, const float *Xs, int32_t S, int32_t d,
+                                const float *params, const int32_t *node, const int32_t *nbr,
+                                int32_t k, float *grad, float *loss) {
+  if (!c || !Xs || !params || !node || !nbr || !grad || S < 2 || d <= 0 || k <= 0)
+    return DRPT_ERR_INVALID_ARG;
+  int nodes = 0;
+  for (int i = 0; i < S; ++i) {
+    if (node[i] < 0 || node[i] >= S) return DRPT_ERR_INVALID_ARG;
+    nodes = std::max(nodes, node[i] + 1);
+  }
+  for (int64_t e = 0; e < (int64_t)S * k; ++e)
+    if (nbr[e] < -1 || nbr[e] >= S) return DRPT_ERR_INVALID_ARG;
+  DRPT_CUDA(cudaSetDevice(c->device));
+  cudaStream_t s = nullptr;
+  LearnArgs a{};
+  DRPT_TRY(learn_buffers(c, 1, S, d, k, nodes, &a));
+  int32_t *perm, *noff, *node_of, *cnt;
+  float *gdev, *acc;
+  DRPT_TRY(ws_get(c, "lg_perm", (size_t)S, &perm));
+  DRPT_TRY(ws_get(c, "lg_noff", (size_t)nodes + 1, &noff));
+  DRPT_TRY(ws_get(c, "lg_node_of", (size_t)S, &node_of));
+  DRPT_TRY(ws_get(c, "lg_cnt", 1, &cnt));
+  DRPT_TRY(ws_get(c, "lg_grad", (size_t)a.np, &gdev));
+  DRPT_TRY(ws_get(c, "lg_loss", 2, &acc));
+  std::vector<int32_t> hp(S), ho(nodes + 1, 0), nb(nbr, nbr + (size_t)S * k), in_ptr, in_idx;
+  for (int i = 0; i < S; ++i) ++ho[node[i] + 1];
+  for (int j = 0; j < nodes; ++j) ho[j + 1] += ho[j];
+  std::vector<int32_t> fill(ho.begin(), ho.end() - 1);
+  for (int i = 0; i < S; ++i) hp[fill[node[i]]++] = i;
+  pair_tables(nb, S, k, &in_ptr, &in_idx);
+  DRPT_CUDA(cudaMemcpy((void *)a.Xs, Xs, (size_t)S * d * 4, cudaMemcpyHostToDevice));
+  DRPT_CUDA(cudaMemcpy(a.params, params, (size_t)a.np * 4, cudaMemcpyHostToDevice));
+  DRPT_CUDA(cudaMemcpy(perm, hp.data(), hp.size() * 4, cudaMemcpyHostToDevice));
+  DRPT_CUDA(cudaMemcpy(noff, ho.data(), ho.size() * 4, cudaMemcpyHostToDevice));
+  DRPT_CUDA(cudaMemcpy(node_of, node, (size_t)S * 4, cudaMemcpyHostToDevice));
+  DRPT_CUDA(cudaMemcpy((void *)a.nbr, nb.data(), nb.size() * 4, cudaMemcpyHostToDevice));
+  DRPT_CUDA(cudaMemcpy((void *)a.in_ptr, in_ptr.data(), in_ptr.size() * 4, cudaMemcpyHostToDevice));
+  if (!in_idx.empty())
+    DRPT_CUDA(cudaMemcpy((void *)a.in_idx, in_idx.data(), in_idx.size() * 4, cudaMemcpyHostToDevice));
+  a.perm = perm;
+  a.noff = noff;
+  a.node_of = node_of;
+  a.nodes = nodes;
+  DRPT_CUDA(cudaMemsetAsync(acc, 0, 2 * sizeof(float), s));
+  DRPT_TRY(launch_learn_pairs(a, cnt, s));
+  DRPT_TRY(launch_learn_step(a, 0.0f, 1.0f, 1.0f, gdev, s));
+  DRPT_TRY(launch_learn_loss(a, acc, 0, s));
+  DRPT_CUDA(cudaMemcpy(grad, gdev, (size_t)a.np * 4, cudaMemcpyDeviceToHost));
+  if (loss) DRPT_CUDA(cudaMemcpy(loss, acc, sizeof(float), cudaMemcpyDeviceToHost));
   return DRPT_OK;
 }
 

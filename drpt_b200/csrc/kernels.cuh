@@ -122,4 +122,49 @@ drpt_status launch_rerank(const void *X, int dtype, int d, const int32_t *visit,
                           const int32_t *cand, int K2, int k, int32_t *out_idx, float *out_dist,
                           cudaStream_t s);
 
+
+// ---- learned splits (k_learned.cu) ------------------------------------------
+constexpr int kLearnHidden = 64;
+constexpr double kLearnEps = 1e-6;  // floor added to a node's variance
+// Training state of one level of T learned trees on a sample of S points.
+// Node tables hold `nodes` entries per tree (noff: nodes + 1), the level's
+// node count.
+struct LearnArgs {
+  const float *Xs;          // S x d standardised sample rows
+  int S, d, T, k;
+  int np;                   // parameters per tree: 64 d + 64 + 64 + 1
+  float *params, *m1, *m2;  // T x np: W1 (64 x d), b1, w2, b2; Adam moments
+  const int32_t *perm;      // T x S: sample ids grouped by node
+  const int32_t *noff;      // T x (nodes + 1) node starts in perm
+  const int32_t *node_of;   // T x S: node of every sample point
+  int nodes;
+  const int32_t *nbr;       // S x k sample-local neighbour ids (-1 = none)
+  const int32_t *in_ptr, *in_idx;  // reverse pairs (CSR over S)
+  const float *inv_pairs;   // T: 1 / (same-node ordered pairs)
+  float *A, *f;             // T x S x 64 activations, T x S outputs
+  float *mu, *var, *sn, *lterm;  // T x nodes node statistics
+  float *g, *sp;            // T x S: dL/df, squared pair sums
+  int R;                    // row chunks of the backward pass
+  float *part;              // T x R x np partial gradients
+};
+drpt_status launch_learn_step(const LearnArgs &a, float lr, float bc1, float bc2, float *grad_out,
+                              cudaStream_t s);
+int learn_step_kernels();
+drpt_status launch_learn_init(const LearnArgs &a, uint64_t seed, int level, cudaStream_t s);
+drpt_status launch_learn_pairs(const LearnArgs &a, int *cnt, cudaStream_t s);
+drpt_status launch_learn_loss(const LearnArgs &a, float *acc, int slot, cudaStream_t s);
+drpt_status launch_gather_f(const LearnArgs &a, float *fp, cudaStream_t s);
+drpt_status launch_node_label(const int32_t *perm, const int32_t *noff, int nodes, int S, int T,
+                              int32_t *node_of, cudaStream_t s);
+drpt_status launch_stack(const LearnArgs &a, int d_pad, int levels, int level,
+                         __nv_bfloat16 *W1b, float *b1, float *w2, float *b2, cudaStream_t s);
+drpt_status launch_sample_scale(const float *Xr, int S, int d, float *c, double *var,
+                                float *inv_sigma, cudaStream_t s);
+drpt_status launch_standardise(const void *X, int dtype, int64_t n, int d, int d_pad,
+                               const int32_t *rows, const float *c, const float *inv_sigma,
+                               __nv_bfloat16 *Xb, float *Xf, cudaStream_t s);
+drpt_status launch_mlp_infer(const __nv_bfloat16 *Xb, int64_t n, int d_pad,
+                             const __nv_bfloat16 *W1b, int nmlp, const float *b1, const float *w2,
+                             const float *b2, float *P, int *err, cudaStream_t s);
+
 }  // namespace drpt

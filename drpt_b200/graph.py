@@ -61,14 +61,18 @@ def global_depth(n: int, tree_depth_ratio: float = 0.6, tree_depth: int = 0) -> 
 def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
                 tree_depth_ratio: float = 0.6, local_tree_offset: int = 2, tree_depth: int = 0,
                 density: float = 0.0, local_seeds=None, device: int = 0, stream=None,
-                out=None, leaf_size: int = 0, precision: str = "bf16"):
+                out=None, leaf_size: int = 0, precision: str = "bf16", learned_trees: int = 0,
+                learn_sample: int = 0, learn_iters: int = 0):
     """k-NN graph of `data` (n x d, uint8 or float32; a NumPy array in host
     memory or a CUDA tensor).  Returns (idx, dist, stats): idx int32 and dist
     float32 of shape (n, nn), each point's nn nearest distinct neighbours other
     than itself over all trees, ordered by (distance, index), -1/+inf padded;
     device tensors when `data` is one.  `out` = (idx, dist) preallocated
     outputs of the same kind as `data`.  `precision` ("bf16" or "fp8") selects
-    the operand type of the mixed form's tensor-core leaf tiles."""
+    the operand type of the mixed form's tensor-core leaf tiles; the last
+    `learned_trees` of the `ntrees` trees split on learned MLP values trained
+    on a sample of `learn_sample` points (0 = 8,192) with `learn_iters` Adam
+    steps per level (0 = 10)."""
     on_dev = _is_cuda_tensor(data)
     if not on_dev:
         data = np.ascontiguousarray(data)
@@ -89,6 +93,8 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
                  "fp32_leaf": _lib.MODE_FP32_LEAF}[mode]
     desc.leaf_size = leaf_size
     desc.precision = {"bf16": _lib.PRECISION_BF16, "fp8": _lib.PRECISION_FP8_E4M3}[precision]
+    desc.learned_trees, desc.learn_sample = learned_trees, learn_sample
+    desc.learn_iters = learn_iters
     desc.data_on_device = 1 if on_dev else 0
     desc.out_on_device = desc.data_on_device
     if on_dev:

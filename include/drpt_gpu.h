@@ -106,6 +106,13 @@ typedef struct {
   int32_t leaf_size;          /* mixed and FP32-leaf modes: target global leaf
                                  size (0 = 512) */
   int32_t precision;          /* mixed mode: drpt_precision of the leaf tiles */
+  int32_t learned_trees;      /* mixed mode: how many of the ntrees (the last
+                                 ones) split on learned MLP values instead of
+                                 random projections (0 = none; d <= 256) */
+  int32_t learn_sample;       /* sample points the split MLPs train on
+                                 (0 = 8,192) */
+  int32_t learn_iters;        /* Adam steps per level (0 = 10) */
+  int32_t reserved;
 } drpt_build_desc;
 
 typedef struct {
@@ -124,6 +131,10 @@ typedef struct {
    * of the BF16 staging kernels; padded Gram-tile multiply-adds per call */
   float ms_leaf_mma, ms_leaf_stage;
   int64_t mma_pairs_padded;
+  /* learned trees: training time (sample neighbours, all levels) and the
+   * mean split loss over trees and levels before and after training */
+  float ms_learn, learn_loss_start, learn_loss_end;
+  int32_t reserved2;
 } drpt_stats;
 
 /* Library version string. */
@@ -182,6 +193,16 @@ typedef struct {
 drpt_status drpt_build_graph_batched(drpt_ctx *ctx, const drpt_batch_desc *desc,
                                      const int64_t *offsets, const void *data, int32_t *out_idx,
                                      float *out_dist, drpt_stats *stats);
+
+/* Loss and gradient of one learned split (no reference counterpart; the
+ * training kernels of the learned trees, one step with learning rate 0).
+ * Host arrays: Xs (S x d sample rows), params (64 d + 129 values: W1 64 x d,
+ * b1 64, w2 64, b2), node (S: node of every sample point, 0 .. S-1), nbr
+ * (S x k sample-local neighbour ids, -1 = none).  Outputs grad (64 d + 129)
+ * and *loss.  The weights are rounded to BF16 in the forward pass. */
+drpt_status drpt_learn_gradient(drpt_ctx *ctx, const float *Xs, int32_t S, int32_t d,
+                                const float *params, const int32_t *node, const int32_t *nbr,
+                                int32_t k, float *grad, float *loss);
 
 /* The reference's sparse Gaussian projection matrix on the host, d x L
  * row-major, from std::mt19937(seed) (math_operations.cpp:48-76). */

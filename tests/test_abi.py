@@ -63,3 +63,29 @@ def test_context_without_device_reports_error():
     h = ctypes.c_void_p()
     st = _lib.load().drpt_ctx_create(ctypes.byref(h), 0)
     assert st in (1, 6)  # invalid device or CUDA error, never a crash
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors of drpt_build_desc, drpt_stats and drpt_batch_desc
+    have the C header's sizes and field offsets (compiled with the system C
+    compiler)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    checks = []
+    for cname, py in (("drpt_build_desc", _lib.BuildDesc), ("drpt_stats", _lib.Stats),
+                      ("drpt_batch_desc", _lib.BatchDesc)):
+        checks.append((f"sizeof({cname})", ctypes.sizeof(py)))
+        for field, _ in py._fields_:
+            checks.append((f"offsetof({cname}, {field})", getattr(py, field).offset))
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "drpt_gpu.h"\nint main(void) {\n' +
+                   "".join(f'  printf("%zu\\n", (size_t){expr});\n' for expr, _ in checks) +
+                   "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    assert got == [v for _, v in checks]
