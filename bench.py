@@ -23,6 +23,17 @@ scaling); the step time is the maximum over ranks.
 --impl reference times the reference's own CPU implementation (the reference
 sources built by `make -C oracle ref`, 1 rank x all host threads) on a
 bounded sample of the same workload.
+
+--workload picks one of the other k-NN-graph workloads (one GPU; the same
+JSON line, with the mixed form's equal-recall FP32 counterpart beside it):
+  ubyte-60k-784   60,000 x 784 uint8 (IDX3-shaped), 10 sparse centres, nn 10
+  fbin-2m-960     2,000,000 x 960 float32, 500 anisotropic Gaussians in
+                  [0,1], nn 20, FP8-E4M3 leaf tiles (BF16 beside)
+  batch-256x96    256 float32 datasets of 96 dims, sizes log-uniform in
+                  [2,000, 200,000], nn 16, one batched build replayed from a
+                  CUDA graph
+  learned-1m-256  1,000,000 x 256 float32 on a 16-dim latent manifold, nn 10,
+                  8 random + 8 learned trees beside 16 and 32 random trees
 """
 from __future__ import annotations
 
@@ -212,6 +223,159 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+
+# ---------------------------------------------------------------- other workloads
+def _timed(fn, steps):
+    """Mean device time (ms) of `steps` calls of fn after one untimed call,
+    CUDA events on the current stream; returns (last result, ms)."""
+    import torch
+    out = fn()
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    for _ in range(steps):
+        out = fn()
+    b.record(s)
+    torch.cuda.synchronize()
+    return out, a.elapsed_time(b) / steps
+
+
+def other_workload(args):
+    import torch
+
+    from drpt_b200 import build_graph, build_graph_batched, recall, synth
+    if _env_int("RANK", 0) != 0:
+        return
+    torch.cuda.set_device(0)
+    steps, warm = args.steps, max(args.warmup, 3)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    wl = args.workload
+    comps = {}
+
+    def rec_of(idx, q, ti, k):
+        return recall.recall_at_k(idx.cpu().numpy()[q][:, :k], ti[:, :k])
+
+    if wl == "batch-256x96":
+        sizes = synth.batch_sizes(256, 2_000, 200_000, seed=4)
+        sets = [synth.batch_dataset(int(m), 96, seed=1000 + i) for i, m in enumerate(sizes)]
+        offs = np.concatenate([[0], np.cumsum([len(x) for x in sets])]).astype(np.int64)
+        X = np.concatenate(sets)
+        n, d, nn, T = len(X), 96, 16, 8
+        Xd = torch.from_numpy(X).cuda()
+        idx = torch.empty((n, nn), dtype=torch.int32, device="cuda")
+        dst = torch.empty((n, nn), dtype=torch.float32, device="cuda")
+
+        def run():
+            return build_graph_batched(Xd, offs, T, nn, SEED_PROJ, mode="mixed", leaf_size=512,
+                                       use_graph=True, out=(idx, dst))[2]
+        for _ in range(warm):
+            run()
+        with ClockSampler(0) as clocks:
+            st, ms = _timed(run, steps)
+        clk = clocks.summary()
+        recs = []
+        for s in range(0, 256, 32):  # every 32nd dataset, 100 queries each
+            x = sets[s]
+            q = recall.sample_queries(len(x), 100, seed=s)
+            ti, _ = recall.exact_knn_fp64(x, q, 10)
+            recs.append(recall.recall_at_k(idx[offs[s]:offs[s + 1]].cpu().numpy()[q][:, :10], ti))
+        rec = float(np.mean(recs))
+        (_, _, st32), ms32 = _timed(lambda: build_graph_batched(Xd, offs, T, nn, SEED_PROJ,
+                                                                mode="fp32_leaf", leaf_size=512), 1)
+        comps["fp32_leaf_batched_same_trees"] = {"points_per_s": n / (ms32 / 1e3), "ms": ms32,
+                                                 "recall@10": rec}
+        comps["mixed_over_plain_fp32_at_equal_recall"] = ms32 / ms
+        cfg = {"workload": "256 float32 datasets, d=96, sizes log-uniform [2000, 200000] "
+                           f"({n} points), 20-200 Gaussians each (sigma 1, centres U[-10,10]); nn=16",
+               "mode": "mixed, batched, CUDA-graph replay", "ntrees": T, "leaf_size": 512,
+               "recall@10": rec, "recall_sample": "100 queries in each of 8 datasets",
+               "kernels_per_build": st.kernels_launched}
+        launches = st.kernels_launched * steps
+        roof = None
+    else:
+        if wl == "ubyte-60k-784":
+            X = synth.clustered_u8(60_000, 784, seed=1)
+            nn, T, leaf, prec, lt = 10, 12, 1024, "bf16", 0
+            desc = "60,000 x 784 uint8 (IDX3-shaped), 10 centres with 80% zero coordinates, sigma 20"
+        elif wl == "fbin-2m-960":
+            X = synth.anisotropic_f32(2_000_000, 960, n_clusters=500, seed=3)
+            nn, T, leaf, prec, lt = 20, 32, 2048, "fp8", 0
+            desc = ("2,000,000 x 960 float32, 500 anisotropic Gaussians (per-dim sigma U[0.01,0.3]), "
+                    "values in [0,1]")
+        else:
+            X = synth.latent_manifold_f32(1_000_000, 256, seed=5)
+            nn, T, leaf, prec, lt = 10, 16, 1024, "bf16", 8
+            desc = "1,000,000 x 256 float32, x = tanh(A z + b) * 4 + N(0, 0.05^2), z ~ N(0, I_16)"
+        n, d = X.shape
+        Xd = torch.from_numpy(X).cuda()
+        del X
+        idx = torch.empty((n, nn), dtype=torch.int32, device="cuda")
+        dst = torch.empty((n, nn), dtype=torch.float32, device="cuda")
+
+        def run(mode="mixed", trees=T, precision=prec, learned=lt, out=(idx, dst)):
+            return build_graph(Xd, trees, nn, SEED_PROJ, mode=mode, leaf_size=leaf,
+                               precision=precision, learned_trees=learned, out=out)[2]
+        for _ in range(warm):
+            run()
+        with ClockSampler(0) as clocks:
+            st, ms = _timed(run, steps)
+        clk = clocks.summary()
+        q = recall.sample_queries(n, 300 if d > 512 else 1000, seed=7)
+        ti, _ = recall.exact_knn_fp64(Xd, q, nn)
+        rec = rec_of(idx, q, ti, 10)
+        cfg = {"workload": desc + f"; nn={nn}", "mode": "mixed", "precision": prec, "ntrees": T,
+               "learned_trees": lt, "leaf_size": leaf, "recall@10": rec,
+               f"recall@{nn}": rec_of(idx, q, ti, nn), "recall_sample": len(q),
+               "phase_ms": {k: getattr(st, "ms_" + k) for k in
+                            ("global", "leaf_knn", "merge", "leaf_mma", "leaf_stage", "learn")}}
+        if lt:
+            cfg["learn_loss"] = [st.learn_loss_start, st.learn_loss_end]
+        launches = st.kernels_launched * steps
+        pi = torch.empty_like(idx)
+        pd = torch.empty_like(dst)
+        others = []
+        if wl == "fbin-2m-960":
+            others.append(("mixed_bf16", dict(precision="bf16")))
+        if lt:
+            others += [(f"mixed_{T}_random_trees", dict(learned=0)),
+                       (f"mixed_{2 * T}_random_trees", dict(trees=2 * T, learned=0)),
+                       (f"fp32_leaf_{2 * T}_random_trees", dict(mode="fp32_leaf", trees=2 * T,
+                                                                  learned=0))]
+        else:
+            others.append((f"fp32_leaf_{T}_trees", dict(mode="fp32_leaf")))
+        for name, kw in others:
+            _, pms = _timed(lambda: run(out=(pi, pd), **kw), 1)
+            comps[name] = {"points_per_s": n / (pms / 1e3), "ms": pms,
+                           "recall@10": rec_of(pi, q, ti, 10)}
+        eq = [v for k, v in comps.items() if k.startswith("fp32") and v["recall@10"] >= rec - 0.01]
+        comps["mixed_over_plain_fp32_at_equal_recall"] = \
+            min(v["ms"] for v in eq) / ms if eq else None
+        mma_ms = st.ms_leaf_mma / T
+        flops = 2.0 * d * st.sum_leaf_sq / T
+        fp8 = prec == "fp8"
+        peak = peaks.get("bf16_tflops_sustained", 1414.3) * (2 if fp8 else 1)
+        roof = {"kernel": f"k_leaf_mma ({'E4M3' if fp8 else 'BF16'} tcgen05 Gram tiles + top-k "
+                          "epilogue), per launch",
+                "bound": "tensor", "achieved": flops / (mma_ms * 1e-3) / 1e12, "peak": peak,
+                "unit": "TFLOP/s", "frac": flops / (mma_ms * 1e-3) / 1e12 / peak, "traffic": None,
+                "peak_source": ("2 x " if fp8 else "") + "MEASURED_PEAKS.json bf16_tflops_sustained "
+                               "(of measured" + ("; FP8 dense rate is twice BF16's)" if fp8 else ")"),
+                "algorithmic_flops_per_launch": flops, "ms_per_launch": mma_ms}
+    cfg["comparisons"] = comps
+    line = {
+        "metric": METRIC, "value": n / (ms / 1e3), "unit": "points/s", "n_gpus": 1,
+        "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8" if wl.startswith("ubyte") else "f32",
+        "data": "synthetic", "config": cfg, "roofline": roof, "cpu_baseline": None,
+        "clocks": clk, "e2e": None, "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
 # ---------------------------------------------------------------- our arm
 def _traffic_per_launch(kernel: str):
     """DRAM bytes per launch of `kernel` from the committed ncu summary."""
@@ -233,9 +397,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain-compare", action="store_true")
+    ap.add_argument("--workload", default="fbin-1m-128",
+                    choices=["fbin-1m-128", "ubyte-60k-784", "fbin-2m-960", "batch-256x96",
+                             "learned-1m-256"])
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.workload != "fbin-1m-128":
+        other_workload(args)
         return
 
     import torch

@@ -330,8 +330,8 @@ drpt_status check_common(const drpt_build_desc *d) {
 // Global depth whose 2^(gd-1) leaves hold at most about `leaf_size` points
 // each (mixed and FP32-leaf modes).
 drpt_status leaf_depth(int64_t n, int leaf_size_in, int *gd_out) {
-  if (leaf_size_in < 0) {
-    set_error("leaf_size %d < 0", leaf_size_in);
+  if (leaf_size_in < 0 || leaf_size_in > 4096) {
+    set_error("leaf_size %d outside [0, 4096]", leaf_size_in);
     return DRPT_ERR_INVALID_ARG;
   }
   const int leaf_size = leaf_size_in > 0 ? leaf_size_in : 512;
@@ -415,6 +415,11 @@ drpt_status mixed_check(drpt_ctx *c, cudaStream_t s) {
   int err = 0;
   DRPT_CUDA(cudaMemcpyAsync(&err, err_d, sizeof(int), cudaMemcpyDeviceToHost, s));
   DRPT_CUDA(cudaStreamSynchronize(s));
+  if (err & 2) {
+    set_error("a global leaf holds more than 8192 points (the tensor-core leaf kernel's limit); "
+              "use a smaller leaf_size");
+    return DRPT_ERR_UNSUPPORTED;
+  }
   if (err) {
     set_error("a bounded wait in the tensor-core leaf kernel gave up");
     return DRPT_ERR_TIMEOUT;

@@ -42,8 +42,20 @@ using namespace sm100;
 
 constexpr int kTM = 128;            // rows per tile (M)
 constexpr int kTN = 64;             // columns per tile (N)
-constexpr int kStages = 2;          // B-tile pipeline depth
-constexpr int kBufCap = 32;         // per-row pending candidates
+// Per list width KP: B-tile stages of the resident-A pipeline, per-row
+// pending-key slots and the CTAs per SM the kernel is built for.  With 16
+// keys per row the epilogue fits 3 CTAs per SM (d <= 128: 66 KB of shared
+// memory each), so one B stage and 32 slots; with 32 keys, 2 CTAs, two
+// stages and 64 slots.
+template <int KP, bool STREAM>
+struct MmaCfg {
+  static constexpr int stages = KP == 16 ? 1 : 2;
+  static constexpr int slots = KP == 16 ? 32 : 64;
+  static constexpr int min_blocks = (KP == 16 && !STREAM) ? 3 : 2;
+};
+constexpr int kColBits = 13;        // low key bits holding the column in the leaf
+constexpr uint32_t kColMask = (1u << kColBits) - 1;
+constexpr int kMaxLeaf = 1 << kColBits;  // largest leaf the key can address
 constexpr int kCheck = 16;          // columns between flush checks
 constexpr int kEpiWarps = 4;
 constexpr int kMmaThreads = 32 * (kEpiWarps + 2);
@@ -307,11 +319,48 @@ __device__ __forceinline__ void bitonic_merge_into(float *L, int32_t *Li, const 
     }
 }
 
+// Sorting networks on single float keys (min / max pairs).
+__device__ __forceinline__ void key_cmp_swap(float *d, int a, int b) {  // d[a] <= d[b]
+  const float x = fminf(d[a], d[b]), y = fmaxf(d[a], d[b]);
+  d[a] = x;
+  d[b] = y;
+}
+
+template <int N>
+__device__ __forceinline__ void key_sort(float *d) {
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1)
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        const int l = i ^ j;
+        if (l > i) {
+          if ((i & k) == 0) key_cmp_swap(d, i, l);
+          else key_cmp_swap(d, l, i);
+        }
+      }
+}
+
+// L (ascending, N) <- the N smallest of L and S (ascending, M <= N).
+template <int N, int M>
+__device__ __forceinline__ void key_merge_into(float *L, const float *S) {
+#pragma unroll
+  for (int i = N - M; i < N; ++i) L[i] = fminf(L[i], S[N - 1 - i]);
+#pragma unroll
+  for (int j = N >> 1; j > 0; j >>= 1)
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      const int l = i ^ j;
+      if (l > i) key_cmp_swap(L, i, l);
+    }
+}
+
 // Shared-memory layout.  Every operand tile is rows of 128 bytes (64 BF16 or
 // 128 E4M3 values of one 128-byte K block), 128-byte swizzled, 1024-byte
 // aligned.
 //   resident A (kb <= 4): A = kb K blocks of the 128 rows, loaded once per row
-//     tile; kStages stages of the kb K blocks of a 64-column B tile;
+//     tile; `stages` stages of the kb K blocks of a 64-column B tile;
 //   streamed A (larger kb): kSStages stages, each one K block of A (16 KB)
 //     and of B (8 KB), so A is re-read from L2 for every column tile.
 constexpr int kSStages = 3;
@@ -321,7 +370,7 @@ struct MmaSmem {
   uint32_t a_off, b_off, buf_off, nrm_off, scl_off, bar_off, total;
 };
 
-__host__ __device__ inline MmaSmem mma_smem_layout(int kb, bool stream) {
+__host__ __device__ inline MmaSmem mma_smem_layout(int kb, bool stream, int stages, int slots) {
   MmaSmem L;
   L.a_off = 0;
   if (stream) {
@@ -329,9 +378,9 @@ __host__ __device__ inline MmaSmem mma_smem_layout(int kb, bool stream) {
     L.buf_off = kSStages * kStreamStage;
   } else {
     L.b_off = L.a_off + (uint32_t)kb * kTM * 128;
-    L.buf_off = L.b_off + (uint32_t)kStages * kb * kTN * 128;
+    L.buf_off = L.b_off + (uint32_t)stages * kb * kTN * 128;
   }
-  L.nrm_off = L.buf_off + kTM * kBufCap * 8;
+  L.nrm_off = L.buf_off + kTM * (uint32_t)slots * 4;
   L.scl_off = L.nrm_off + kEpiWarps * kTN * 4;
   L.bar_off = L.scl_off + kEpiWarps * kTN * 4;
   L.total = L.bar_off + 16 * 8 + 16;
@@ -342,7 +391,7 @@ __host__ __device__ inline MmaSmem mma_smem_layout(int kb, bool stream) {
 // operands with per-row scales `scl` (scores are then scaled by the row's and
 // the column's scale); otherwise BF16.
 template <int KP, bool STREAM, bool FP8>
-__global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
+__global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks)) k_leaf_mma(
     const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
     const int32_t *__restrict__ goff, const int32_t *__restrict__ order,
     const float *__restrict__ nrm, const float *__restrict__ scl,
@@ -352,22 +401,24 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
-  const MmaSmem L = mma_smem_layout(kb, STREAM);
+  using Cfg = MmaCfg<KP, STREAM>;
+  constexpr int kBufSlots = Cfg::slots;
+  const MmaSmem L = mma_smem_layout(kb, STREAM, Cfg::stages, Cfg::slots);
   uint8_t *sA = smem + L.a_off;
   uint8_t *sB = smem + L.b_off;
-  uint2 *buf = reinterpret_cast<uint2 *>(smem + L.buf_off);  // [slot][row]: (value bits, position)
+  uint32_t *buf = reinterpret_cast<uint32_t *>(smem + L.buf_off);  // [slot][row] keys
   float *nbuf = reinterpret_cast<float *>(smem + L.nrm_off);  // [warp][kTN] column norms of a tile
   float *sbuf = reinterpret_cast<float *>(smem + L.scl_off);  // [warp][kTN] column scales (FP8)
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L.bar_off);
-  constexpr int kMaxStages = kStages > kSStages ? kStages : kSStages;
+  static_assert(kSStages <= 3 && Cfg::stages <= 3, "barrier slots");
   uint64_t *full_a = bars + 0;
-  uint64_t *full_b = bars + 1;                // kMaxStages
-  uint64_t *empty_b = bars + 1 + kMaxStages;  // kMaxStages
-  uint64_t *acc_full = bars + 1 + 2 * kMaxStages;
+  uint64_t *full_b = bars + 1;       // up to 3 stages
+  uint64_t *empty_b = bars + 1 + 3;  // up to 3 stages
+  uint64_t *acc_full = bars + 1 + 2 * 3;
   uint64_t *acc_empty = acc_full + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 16);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 16) + 1;
-  constexpr int NS = STREAM ? kSStages : kStages;
+  constexpr int NS = STREAM ? kSStages : Cfg::stages;
   constexpr int kKE = FP8 ? 128 : 64;  // elements per 128-byte K block
 
   const int u = blockIdx.x;
@@ -375,6 +426,10 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int leaf = tile_leaf[u], r0 = tile_r0[u];
   const int32_t lo = goff[leaf], m = goff[leaf + 1] - lo;
+  if (m > kMaxLeaf) {  // the candidate keys address at most kMaxLeaf columns
+    if (threadIdx.x == 0) atomicOr(err, 2);
+    return;  // uniform for the whole block
+  }
   const int nct = (m + kTN - 1) / kTN;
   const uint32_t a_bytes = (uint32_t)kb * kTM * 128, b_bytes = (uint32_t)kb * kTN * 128;
 
@@ -485,20 +540,20 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
       if (!ok) *abort_flag = 1;
     }
   } else {
-    // ---- epilogue: thread = row (TMEM lane).  Candidates below the row's
-    // current KP-th best go to a slot-major shared buffer (conflict-free:
-    // consecutive rows are consecutive words); when any row of the warp has
-    // kCheck pending, every row sorts its pending entries in batches of 16
-    // and merges them into its sorted list with a bitonic network.
+    // ---- epilogue: thread = row (TMEM lane).  A candidate is one 32-bit
+    // key: its score (an FP32 value, ordered as a float) with the low
+    // kColBits mantissa bits replaced by its column in the leaf, so keys sort
+    // with plain min/max and equal scores order by column.  Keys below the
+    // row's current KP-th best go to a slot-major shared buffer
+    // (conflict-free: consecutive rows are consecutive words); when any row
+    // of the warp has too many pending, every row sorts its pending keys in
+    // batches of 16 and merges them into its sorted list of KP keys with a
+    // bitonic network.
     const int row = warp * 32 + lane;
     const bool rvalid = r0 + row < m;
     float td[KP];
-    int32_t ti[KP];
 #pragma unroll
-    for (int j = 0; j < KP; ++j) {
-      td[j] = __int_as_float(0x7f800000);
-      ti[j] = -1;
-    }
+    for (int j = 0; j < KP; ++j) td[j] = __int_as_float(0x7f800000);
     // Candidates that cannot beat the KP-th of the point's running list
     // (approximate squared distances of the earlier trees) are never kept.
     // (rows past the leaf get -inf and keep nothing)
@@ -513,53 +568,58 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
       if (tree > 0) thr = run_dist[(int64_t)my_pt * KP + KP - 1] - nr;
     }
     const float thr0 = thr;
-    // Pending candidates: a passing candidate is stored at the next free slot
-    // of one of two per-row lanes of the buffer (even and odd columns, so two
-    // independent append chains) by a predicated shared-memory store, no
-    // branch; slot addresses are 32-bit shared-window offsets.
-    constexpr int kHalf = kBufCap / 2;
-    uint2 *const pbase = buf + row;
-    const uint32_t abase0 = smem_u32(pbase), abase1 = abase0 + kHalf * kTM * 8;
-    uint32_t aslot0 = abase0, aslot1 = abase1;
-    auto pending0 = [&]() { return (int)((aslot0 - abase0) / (kTM * 8)); };
-    auto pending1 = [&]() { return (int)((aslot1 - abase1) / (kTM * 8)); };
+    const uint32_t my_col = (uint32_t)(r0 + row);  // the row's own point, dropped when read
+    // Pending keys: a passing key is stored at the next free slot of one of
+    // two per-row lanes of the buffer (even and odd columns, two independent
+    // append chains) by a predicated shared-memory store, no branch; slot
+    // addresses are 32-bit shared-window offsets.
+    constexpr int kChains = 2, kLane = kBufSlots / kChains, kPerBatch = 16 / kChains;
+    uint32_t *const pbase = buf + row;
+    const uint32_t abase = smem_u32(pbase);
+    uint32_t aslot[kChains];
+#pragma unroll
+    for (int q = 0; q < kChains; ++q) aslot[q] = abase + q * kLane * kTM * 4;
+    auto pending = [&](int q) {
+      return (int)((aslot[q] - abase - q * kLane * kTM * 4) / (kTM * 4));
+    };
     auto flush = [&]() {
-      const int c0 = pending0(), c1 = pending1();
-      const int mx = __reduce_max_sync(kFull, max(c0, c1));
-      for (int base = 0; base < mx; base += 8) {
-        // 8 slots of each half make one batch of 16
+      int cnt[kChains], mine = 0;
+#pragma unroll
+      for (int q = 0; q < kChains; ++q) {
+        cnt[q] = pending(q);
+        mine = max(mine, cnt[q]);
+      }
+      const int mx = __reduce_max_sync(kFull, mine);
+      for (int base = 0; base < mx; base += kPerBatch) {
         float sd[16];
-        int32_t si[16];
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
-          const int half = e >> 3, slot = base + (e & 7);
-          const bool have = slot < (half ? c1 : c0);
-          const uint2 ent = have ? pbase[(half * kHalf + slot) * kTM]
-                                 : make_uint2(0x7f800000u, 0xffffffffu);
-          sd[e] = __uint_as_float(ent.x);
-          si[e] = (int32_t)ent.y;
+          const int q = e / kPerBatch, slot = base + e % kPerBatch;
+          uint32_t key = 0x7f800000u;
+          if (slot < cnt[q]) key = pbase[(q * kLane + slot) * kTM];
+          if ((key & kColMask) == my_col && key != 0x7f800000u) key = 0x7f800000u;
+          sd[e] = __uint_as_float(key);
         }
-        bitonic_sort<16>(sd, si);
-        bitonic_merge_into<KP, 16>(td, ti, sd, si);
+        key_sort<16>(sd);
+        key_merge_into<KP, 16>(td, sd);
       }
-      aslot0 = abase0;
-      aslot1 = abase1;
+#pragma unroll
+      for (int q = 0; q < kChains; ++q) aslot[q] = abase + q * kLane * kTM * 4;
       thr = fminf(thr0, td[KP - 1]);
     };
-    auto append = [&](uint32_t &aslot, float sv, uint32_t pos) {
+    auto append = [&](uint32_t &slot, float sv, uint32_t col) {
+      const uint32_t key = (__float_as_uint(sv) & ~kColMask) | col;
       asm volatile(
           "{\n\t.reg .pred p;\n\t"
           "setp.lt.f32 p, %1, %2;\n\t"
-          "@p st.shared.v2.u32 [%0], {%3, %4};\n\t"
-          "@p add.u32 %0, %0, %5;\n\t}"
-          : "+r"(aslot)
-          : "f"(sv), "f"(thr), "r"(__float_as_uint(sv)), "r"(pos), "n"(kTM * 8)
+          "@p st.shared.u32 [%0], %3;\n\t"
+          "@p add.u32 %0, %0, %4;\n\t}"
+          : "+r"(slot)
+          : "f"(sv), "f"(thr), "r"(key), "n"(kTM * 4)
           : "memory");
     };
-    // one 32-column chunk of scores; DIAG: the warp's diagonal chunk, where
-    // lane l's own point is column l and is skipped
-    auto scan = [&](const float *v, const float *wn, const float *ws, int cb, auto diag_tag) {
-      constexpr bool DIAG = decltype(diag_tag)::value;
+    // one 32-column chunk of scores starting at leaf column cb
+    auto scan = [&](const float *v, const float *wn, const float *ws, uint32_t cb) {
 #pragma unroll
       for (int h = 0; h < 32; h += kCheck) {
 #pragma unroll
@@ -576,71 +636,101 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_leaf_mma(
             float sv;
             if constexpr (FP8) sv = fmaf(m2s * scs[e], v[j], ncs[e]);
             else sv = fmaf(-2.0f, v[j], ncs[e]);
-            if (DIAG) sv = (j == lane) ? __int_as_float(0x7f800000) : sv;
-            if (j & 1) append(aslot1, sv, (uint32_t)(cb + j));
-            else append(aslot0, sv, (uint32_t)(cb + j));
+            append(aslot[j % kChains], sv, cb + (uint32_t)j);
           }
         }
-        if (__any_sync(kFull, max(pending0(), pending1()) >= kHalf - kCheck / 2)) flush();
+        int most = 0;
+#pragma unroll
+        for (int q = 0; q < kChains; ++q) most = max(most, pending(q));
+        if (__any_sync(kFull, most > kLane - kCheck / kChains)) flush();
       }
     };
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    // column norms (and E4M3 scales) of a tile: lane l holds columns l and
+    // l + 32, loaded one tile ahead; columns past the leaf carry an infinite
+    // norm and so never pass
+    float pn[kTN / 32], ps[kTN / 32];
+    auto load_cols = [&](int c) {
+#pragma unroll
+      for (int h = 0; h < kTN / 32; ++h) {
+        const int col = c * kTN + h * 32 + lane;
+        const bool in = c < nct && col < m;
+        pn[h] = in ? __ldg(nrm + lo + col) : __int_as_float(0x7f800000);
+        ps[h] = 0.0f;
+        if constexpr (FP8) ps[h] = in ? __ldg(scl + lo + col) : 0.0f;
+      }
+    };
+    load_cols(0);
     for (int c = 0; c < nct; ++c) {
       const int b = c & 1;
+      // this tile's column norms, staged per warp (16-byte aligned reads)
+      float *wn = nbuf + warp * kTN;
+      float *ws = sbuf + warp * kTN;
+      __syncwarp();
+#pragma unroll
+      for (int h = 0; h < kTN / 32; ++h) {
+        wn[h * 32 + lane] = pn[h];
+        if constexpr (FP8) ws[h * 32 + lane] = ps[h];
+      }
+      __syncwarp();
+      load_cols(c + 1);
       if (!__all_sync(kFull, mbar_wait(acc_full + b, (c >> 1) & 1))) {
         *abort_flag = 1;
         break;
       }
       tc_fence_after();
-      // this tile's column norms, staged per warp (16-byte aligned reads);
-      // columns past the leaf carry an infinite norm and so never pass
-      float *wn = nbuf + warp * kTN;
-      float *ws = sbuf + warp * kTN;
-      __syncwarp();
-#pragma unroll
-      for (int h = 0; h < kTN; h += 32) {
-        const int col = c * kTN + h + lane;
-        wn[h + lane] = col < m ? __ldg(nrm + lo + col) : __int_as_float(0x7f800000);
-        if constexpr (FP8) ws[h + lane] = col < m ? __ldg(scl + lo + col) : 0.0f;
-      }
-      __syncwarp();
 #pragma unroll
       for (int q = 0; q < kTN / 32; ++q) {
         float v[32];
         tmem_ld32(lane_base + b * kTN + q * 32, v);
-        const int cb = c * kTN + q * 32;
-        // the warp's 32 rows sit in one 32-column chunk of the diagonal
-        if (cb == r0 + warp * 32)
-          scan(v, wn + q * 32, ws + q * 32, lo + cb, std::true_type{});
-        else
-          scan(v, wn + q * 32, ws + q * 32, lo + cb, std::false_type{});
+        scan(v, wn + q * 32, ws + q * 32, (uint32_t)(c * kTN + q * 32));
       }
       tc_fence_before();
       mbar_arrive(acc_empty + b);
     }
     flush();
     if (rvalid) {
-      // fold this tree's list into the running list: drop neighbours it
-      // already holds, then a bitonic merge keeps the KP best
+      // fold this tree's list into the running list: keys back to (squared
+      // distance, point id); drop neighbours the running list already holds;
+      // a bitonic merge keeps the KP best by (distance, id)
       const int64_t o = (int64_t)my_pt * KP;
       float rd[KP];
       int32_t ri[KP];
 #pragma unroll
       for (int j = 0; j < KP; ++j) {
-        rd[j] = tree > 0 ? run_dist[o + j] : __int_as_float(0x7f800000);
-        ri[j] = tree > 0 ? run_idx[o + j] : -1;
+        const uint32_t key = __float_as_uint(td[j]);
+        const bool have = key != 0x7f800000u;
+        const int32_t q = have ? __ldg(order + lo + (int32_t)(key & kColMask)) : -1;
+        rd[j] = have ? nr + __uint_as_float(key & ~kColMask) : __int_as_float(0x7f800000);
+        ri[j] = q;
       }
+      if (tree > 0) {
+        float od[KP];
+        int32_t oi[KP];
 #pragma unroll
-      for (int j = 0; j < KP; ++j) {
-        int32_t q = ti[j] >= 0 ? __ldg(order + ti[j]) : -1;
-        bool dup = false;
+        for (int j = 0; j < KP; ++j) {
+          od[j] = run_dist[o + j];
+          oi[j] = run_idx[o + j];
+        }
 #pragma unroll
-        for (int i = 0; i < KP; ++i) dup |= (q >= 0 && ri[i] == q);
-        ti[j] = dup ? -1 : q;
-        td[j] = (dup || q < 0) ? __int_as_float(0x7f800000) : nr + td[j];
+        for (int j = 0; j < KP; ++j) {
+          bool dup = false;
+#pragma unroll
+          for (int i = 0; i < KP; ++i) dup |= (ri[j] >= 0 && oi[i] == ri[j]);
+          if (dup) {
+            ri[j] = -1;
+            rd[j] = __int_as_float(0x7f800000);
+          }
+        }
+        bitonic_sort<KP>(rd, ri);
+        bitonic_merge_into<KP, KP>(od, oi, rd, ri);
+#pragma unroll
+        for (int j = 0; j < KP; ++j) {
+          rd[j] = od[j];
+          ri[j] = oi[j];
+        }
       }
-      bitonic_sort<KP>(td, ti);
-      bitonic_merge_into<KP, KP>(rd, ri, td, ti);
+      // (tree 0: the list is already ascending by key, i.e. by distance)
 #pragma unroll
       for (int j = 0; j < KP; ++j) {
         run_dist[o + j] = rd[j];
@@ -874,7 +964,8 @@ void center_d(const MixedTreeArgs &a, cudaStream_t s) {
 template <int KP, bool STREAM, bool FP8>
 drpt_status mma_t(const MixedTreeArgs &a, const CUtensorMap &tmA, const CUtensorMap &tmB, int kb,
                   cudaStream_t s) {
-  const MmaSmem L = mma_smem_layout(kb, STREAM);
+  const MmaSmem L = mma_smem_layout(kb, STREAM, MmaCfg<KP, STREAM>::stages,
+                                    MmaCfg<KP, STREAM>::slots);
   const size_t smem = L.total + 1024;
   if (smem > 227 * 1024) {
     set_error("mixed leaf kernel: %zu bytes of shared memory needed", smem);
