@@ -359,7 +359,7 @@ __device__ __forceinline__ void key_merge_into(float *L, const float *S) {
 // Shared-memory layout.  Every operand tile is rows of 128 bytes (64 BF16 or
 // 128 E4M3 values of one 128-byte K block), 128-byte swizzled, 1024-byte
 // aligned.
-//   resident A (kb <= 4): A = kb K blocks of the 128 rows, loaded once per row
+//   resident A (kb <= 2): A = kb K blocks of the 128 rows, loaded once per row
 //     tile; `stages` stages of the kb K blocks of a 64-column B tile;
 //   streamed A (larger kb): kSStages stages, each one K block of A (16 KB)
 //     and of B (8 KB), so A is re-read from L2 for every column tile.
@@ -984,7 +984,9 @@ drpt_status mma_t(const MixedTreeArgs &a, const CUtensorMap &tmA, const CUtensor
 template <int KP>
 drpt_status mma_kp(const MixedTreeArgs &a, const CUtensorMap &tmA, const CUtensorMap &tmB, int kb,
                    cudaStream_t s) {
-  const bool stream = kb > 4;
+  // Resident A only for up to two K blocks: beyond that the streamed
+  // stages fit two CTAs per SM where a resident A tile fits one.
+  const bool stream = kb > 2;
   if (a.fp8)
     return stream ? mma_t<KP, true, true>(a, tmA, tmB, kb, s) : mma_t<KP, false, true>(a, tmA, tmB, kb, s);
   return stream ? mma_t<KP, true, false>(a, tmA, tmB, kb, s) : mma_t<KP, false, false>(a, tmA, tmB, kb, s);

@@ -18,6 +18,15 @@ constexpr int kThreads = 256;
 template <typename T>
 __device__ __forceinline__ float to_f(T v) { return (float)v; }
 
+// Four consecutive elements (16-byte or 4-byte aligned: d % 4 == 0) as floats.
+__device__ __forceinline__ float4 load4v(const float *p) {
+  return __ldg(reinterpret_cast<const float4 *>(p));
+}
+__device__ __forceinline__ float4 load4v(const uint8_t *p) {
+  const uchar4 q = __ldg(reinterpret_cast<const uchar4 *>(p));
+  return make_float4(q.x, q.y, q.z, q.w);
+}
+
 // Block: `pts` consecutive points (or the block table's entry: first point,
 // points, column set); thread pairs (point, column) with the point index
 // fastest so a warp writes 32 consecutive P entries of a column.
@@ -34,22 +43,46 @@ __global__ void __launch_bounds__(kThreads) k_project(const T *__restrict__ X, i
     csc.colptr += (int64_t)b[2] * (csc.ncols + 1);
   }
   const int ld = d + 1;
-  // Stage the rows: consecutive threads read consecutive elements of a row.
-  const int total = np * d;
   const T *src = X + p0 * d;
-  for (int e = threadIdx.x; e < total; e += kThreads) {
-    const int r = e / d, c = e - r * d;
-    xs[r * ld + c] = to_f(src[e]);
+  if (d % 4 == 0) {
+    // Stage the rows with 4-element loads: warp w takes rows w, w + 8, ...,
+    // lane l the quads l, l + 32, ... of a row (no index division).
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, q4 = d >> 2;
+#pragma unroll 2
+    for (int r = warp; r < np; r += kThreads / 32) {
+      const T *row = src + (int64_t)r * d;
+      float *dst = xs + r * ld;
+      for (int c4 = lane; c4 < q4; c4 += 32) {
+        const float4 v = load4v(row + 4 * c4);
+        dst[4 * c4] = v.x;
+        dst[4 * c4 + 1] = v.y;
+        dst[4 * c4 + 2] = v.z;
+        dst[4 * c4 + 3] = v.w;
+      }
+    }
+  } else {
+    // consecutive threads read consecutive elements of a row
+    const int total = np * d;
+    for (int e = threadIdx.x; e < total; e += kThreads) {
+      const int r = e / d, c = e - r * d;
+      xs[r * ld + c] = to_f(src[e]);
+    }
   }
   __syncthreads();
+  // pairs q = col * np + r, walked in steps of the block size without division
   const int pairs = np * csc.ncols;
+  int col = threadIdx.x / np, r = threadIdx.x - col * np;
   for (int q = threadIdx.x; q < pairs; q += kThreads) {
-    const int col = q / np, r = q - col * np;
     const int e0 = __ldg(csc.colptr + col), e1 = __ldg(csc.colptr + col + 1);
     const float *x = xs + r * ld;
     float acc = 0.0f;
     for (int e = e0; e < e1; ++e) acc = __fadd_rn(acc, __fmul_rn(x[__ldg(csc.row + e)], __ldg(csc.val + e)));
     P[(int64_t)col * n + p0 + r] = acc;
+    r += kThreads;
+    while (r >= np) {
+      r -= np;
+      ++col;
+    }
   }
 }
 
