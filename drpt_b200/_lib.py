@@ -27,7 +27,8 @@ EXPORTS = [
     "drpt_version", "drpt_last_error", "drpt_ctx_create", "drpt_ctx_destroy", "drpt_build_graph",
     "drpt_host_projection", "drpt_project", "drpt_global_trees", "drpt_local_leaves",
     "drpt_leaf_knn", "drpt_merge_candidates", "drpt_global_trees_noalloc",
-    "drpt_build_graph_batched", "drpt_learn_gradient",
+    "drpt_build_graph_batched", "drpt_learn_gradient", "drpt_index_build", "drpt_index_query",
+    "drpt_index_destroy",
 ]
 
 
@@ -115,12 +116,18 @@ def load(path: str = LIB_PATH):
         L.drpt_leaf_knn.argtypes = [vp, vp, i32, i64, i32, i32, vp, vp, i32, i32, vp, vp, vp]
         L.drpt_merge_candidates.argtypes = [vp, vp, vp, i64, i32, i32, vp, vp, vp]
         L.drpt_global_trees_noalloc.argtypes = [vp, i64, i32, i32, i32, vp, vp, vp, vp]
+        L.drpt_index_build.argtypes = [vp, ctypes.POINTER(BuildDesc), vp, vp, vp,
+                                       ctypes.POINTER(Stats), ctypes.POINTER(vp)]
+        L.drpt_index_query.argtypes = [vp, vp, i64, i32, i32, vp, vp, vp]
+        L.drpt_index_destroy.argtypes = [vp]
+        L.drpt_index_destroy.restype = None
         L.drpt_learn_gradient.argtypes = [vp, vp, i32, i32, vp, vp, vp, i32, vp, vp]
         L.drpt_build_graph_batched.argtypes = [vp, ctypes.POINTER(BatchDesc), vp, vp, vp, vp,
                                                ctypes.POINTER(Stats)]
         for name in EXPORTS:
             fn = getattr(L, name)
-            if name not in ("drpt_version", "drpt_last_error", "drpt_ctx_destroy"):
+            if name not in ("drpt_version", "drpt_last_error", "drpt_ctx_destroy",
+                            "drpt_index_destroy"):
                 fn.restype = ctypes.c_int
         _lib = L
         return L

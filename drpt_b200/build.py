@@ -75,7 +75,8 @@ def build_cli(force: bool = False) -> str:
     if not force and not _stale(CLI, deps):
         return CLI
     cmd = [_host_cxx(), "-std=c++17", "-O2", "-I" + INCLUDE, "-I/usr/local/cuda/include", src,
-           "-o", CLI, "-L" + PKG, "-ldrpt_gpu", "-Wl,-rpath,$ORIGIN"]
+           "-o", CLI, "-L" + PKG, "-ldrpt_gpu", "-Wl,-rpath,$ORIGIN", "-Wl,-Bstatic", "-lz",
+           "-Wl,-Bdynamic"]
     subprocess.run(cmd, check=True)
     return CLI
 

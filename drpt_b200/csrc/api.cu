@@ -45,6 +45,32 @@ struct drpt_ctx {
   int glaunches = 0;
 };
 
+// A built mixed-form index kept for out-of-sample queries: its own copies of
+// the rows, every tree's leaf order, leaf starts and node medians, and the
+// split functions (the random trees' projection columns as CSC, the learned
+// trees' MLPs and standardisation).  Device memory owned by the index.
+struct drpt_index {
+  int device = 0;
+  int64_t n = 0;
+  int d = 0, dtype = 0, T = 0, gd = 0, nleaf = 0, Tr = 0, Tl = 0, d_pad = 0;
+  void *X = nullptr;
+  int32_t *order = nullptr, *goff = nullptr;
+  float *medians = nullptr;
+  int32_t *csc_col = nullptr, *csc_row = nullptr;
+  float *csc_val = nullptr;
+  int ncols_r = 0;
+  __nv_bfloat16 *w1b = nullptr;
+  float *b1 = nullptr, *w2 = nullptr, *b2 = nullptr, *c = nullptr, *inv_sigma = nullptr;
+  // query scratch, grown on demand
+  int64_t cap = 0;
+  float *Pq = nullptr;
+  int32_t *leaf = nullptr, *qi = nullptr;
+  float *qd = nullptr;
+  void *qx = nullptr;
+  __nv_bfloat16 *qxb = nullptr;
+  int *err = nullptr;
+};
+
 namespace drpt {
 
 static thread_local char g_err[1024] = "";
@@ -100,7 +126,8 @@ drpt_status geometry(int64_t n, int tree_depth, double ratio, Geometry *g) {
 
 // K1 with the CSC of the used columns of B built on the host.
 drpt_status project_cols(drpt_ctx *c, const void *X, int dtype, int64_t n, int d, const float *B,
-                         int L, const std::vector<int32_t> &cols, float *P, cudaStream_t s) {
+                         int L, const std::vector<int32_t> &cols, float *P, cudaStream_t s,
+                         int *nnz_out = nullptr) {
   const int ncols = (int)cols.size();
   std::vector<int32_t> colptr(ncols + 1, 0), row;
   std::vector<float> val;
@@ -125,6 +152,7 @@ drpt_status project_cols(drpt_ctx *c, const void *X, int dtype, int64_t n, int d
     DRPT_CUDA(cudaMemcpyAsync(drow, row.data(), row.size() * 4, cudaMemcpyHostToDevice, s));
     DRPT_CUDA(cudaMemcpyAsync(dval, val.data(), val.size() * 4, cudaMemcpyHostToDevice, s));
   }
+  if (nnz_out) *nnz_out = (int)row.size();
   CscDev csc{dcol, drow, dval, ncols};
   DRPT_TRY(launch_project(X, dtype, n, d, csc, P, s));
   c->launches += 1;
@@ -684,8 +712,16 @@ drpt_status learn_and_project(drpt_ctx *c, const void *X, int dtype, int64_t n, 
 // statistics grown to leaves of about `leaf_size` points, BF16 tensor-core
 // brute force of every global leaf, cross-tree merge of the approximate
 // candidates, exact FP32 re-rank with the FP64 boundary check.
+template <typename Tp>
+drpt_status dev_copy(Tp **dst, const void *src, size_t count, cudaStream_t s) {
+  const size_t bytes = std::max<size_t>(count * sizeof(Tp), 4);
+  DRPT_CUDA(cudaMalloc((void **)dst, bytes));
+  if (count) DRPT_CUDA(cudaMemcpyAsync(*dst, src, count * sizeof(Tp), cudaMemcpyDeviceToDevice, s));
+  return DRPT_OK;
+}
+
 drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, int32_t *oi,
-                      float *od, drpt_stats *stats, cudaStream_t s) {
+                      float *od, drpt_stats *stats, cudaStream_t s, drpt_index *keep = nullptr) {
   const int64_t n = desc->n;
   const int d = desc->d, T = desc->ntrees, nn = desc->nn;
   if (nn > 32) {
@@ -728,7 +764,9 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
     for (int l = 0; l + 1 < gd; ++l) cols.push_back(t * gd + l);
   float *P = nullptr;
   DRPT_TRY(ws_get(c, "P", std::max<size_t>((size_t)T * (gd - 1), 1) * n, &P));
-  if (!cols.empty()) DRPT_TRY(project_cols(c, X, desc->dtype, n, d, B.data(), L, cols, P, s));
+  int nnz = 0;
+  if (!cols.empty())
+    DRPT_TRY(project_cols(c, X, desc->dtype, n, d, B.data(), L, cols, P, s, &nnz));
   LearnResult lres;
   float ms_learn = 0.0f;
   if (learned > 0) {
@@ -740,12 +778,60 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
         std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
   int32_t *order, *goff;
-  DRPT_TRY(global_trees(c, P, n, T, gd, 0, nullptr, &order, &goff, s));
+  float *medians = nullptr;
+  if (keep) DRPT_TRY(ws_get(c, "medians", (size_t)T * std::max(nleaf - 1, 1), &medians));
+  DRPT_TRY(global_trees(c, P, n, T, gd, 0, medians, &order, &goff, s));
   DRPT_CUDA(cudaEventRecord(ev[2], s));
 
   DRPT_TRY(mixed_leaf_phase(c, X, desc->dtype, n, d, T, nn, fp8, order, goff, nleaf, oi, od,
                             /*timed=*/true, s));
   DRPT_TRY(mixed_check(c, s));
+  if (keep) {
+    // the index keeps its own copies: the workspace is reused by later calls
+    keep->n = n;
+    keep->d = d;
+    keep->dtype = desc->dtype;
+    keep->T = T;
+    keep->gd = gd;
+    keep->nleaf = nleaf;
+    keep->Tr = Tr;
+    keep->Tl = learned;
+    keep->d_pad = (d + 63) / 64 * 64;
+    const size_t esz = desc->dtype == DRPT_DTYPE_U8 ? 1 : 4;
+    DRPT_TRY(dev_copy((uint8_t **)&keep->X, X, (size_t)n * d * esz, s));
+    DRPT_TRY(dev_copy(&keep->order, order, (size_t)T * n, s));
+    DRPT_TRY(dev_copy(&keep->goff, goff, (size_t)T * (nleaf + 1), s));
+    DRPT_TRY(dev_copy(&keep->medians, medians, (size_t)T * std::max(nleaf - 1, 1), s));
+    keep->ncols_r = (int)cols.size();
+    if (!cols.empty()) {
+      int32_t *dcol, *drow;
+      float *dval;
+      DRPT_TRY(ws_get(c, "csc_colptr", cols.size() + 1, &dcol));
+      DRPT_TRY(ws_get(c, "csc_row", std::max<size_t>(nnz, 1), &drow));
+      DRPT_TRY(ws_get(c, "csc_val", std::max<size_t>(nnz, 1), &dval));
+      DRPT_TRY(dev_copy(&keep->csc_col, dcol, cols.size() + 1, s));
+      DRPT_TRY(dev_copy(&keep->csc_row, drow, (size_t)nnz, s));
+      DRPT_TRY(dev_copy(&keep->csc_val, dval, (size_t)nnz, s));
+    }
+    if (learned > 0) {
+      const size_t M = (size_t)learned * (gd - 1);
+      __nv_bfloat16 *wb;
+      float *b1, *w2, *b2, *cc, *is;
+      DRPT_TRY(ws_get(c, "ln_w1b", M * kLearnHidden * keep->d_pad, &wb));
+      DRPT_TRY(ws_get(c, "ln_b1", M * kLearnHidden, &b1));
+      DRPT_TRY(ws_get(c, "ln_w2", M * kLearnHidden, &w2));
+      DRPT_TRY(ws_get(c, "ln_b2", M, &b2));
+      DRPT_TRY(ws_get(c, "ln_c", (size_t)d, &cc));
+      DRPT_TRY(ws_get(c, "ln_inv_sigma", 1, &is));
+      DRPT_TRY(dev_copy(&keep->w1b, wb, M * kLearnHidden * keep->d_pad, s));
+      DRPT_TRY(dev_copy(&keep->b1, b1, M * kLearnHidden, s));
+      DRPT_TRY(dev_copy(&keep->w2, w2, M * kLearnHidden, s));
+      DRPT_TRY(dev_copy(&keep->b2, b2, M, s));
+      DRPT_TRY(dev_copy(&keep->c, cc, (size_t)d, s));
+      DRPT_TRY(dev_copy(&keep->inv_sigma, is, 1, s));
+    }
+    DRPT_CUDA(cudaStreamSynchronize(s));
+  }
   if (stats) {
     std::memset(stats, 0, sizeof(*stats));
     stats->tree_depth = gd;
@@ -1343,8 +1429,9 @@ drpt_status drpt_host_projection(uint32_t seed, int32_t d, int32_t L, float dens
   return DRPT_OK;
 }
 
-drpt_status drpt_build_graph(drpt_ctx *c, const drpt_build_desc *desc, const void *data,
-                             int32_t *out_idx, float *out_dist, drpt_stats *stats) {
+static drpt_status build_graph_impl(drpt_ctx *c, const drpt_build_desc *desc, const void *data,
+                                    int32_t *out_idx, float *out_dist, drpt_stats *stats,
+                                    drpt_index *keep) {
   if (!c || !data || !out_idx) return DRPT_ERR_INVALID_ARG;
   DRPT_TRY(check_common(desc));
   DRPT_CUDA(cudaSetDevice(c->device));
@@ -1387,7 +1474,7 @@ drpt_status drpt_build_graph(drpt_ctx *c, const drpt_build_desc *desc, const voi
     } else if (!od) {
       DRPT_TRY(ws_get(c, "out_dist", (size_t)n * nn, &od));
     }
-    if (desc->mode == DRPT_MODE_MIXED) DRPT_TRY(run_mixed(c, desc, X, oi, od, stats, s));
+    if (desc->mode == DRPT_MODE_MIXED) DRPT_TRY(run_mixed(c, desc, X, oi, od, stats, s, keep));
     else DRPT_TRY(run_fp32_leaf(c, desc, X, oi, od, stats, s));
     if (!desc->out_on_device) {
       DRPT_CUDA(cudaMemcpyAsync(out_idx, oi, (size_t)n * nn * 4, cudaMemcpyDeviceToHost, s));
@@ -1478,6 +1565,113 @@ drpt_status drpt_build_graph(drpt_ctx *c, const drpt_build_desc *desc, const voi
     stats->ms_merge = elapsed(ev[4], ev[5]);
     stats->ms_total = elapsed(ev[0], ev[6]);
   }
+  return DRPT_OK;
+}
+
+drpt_status drpt_build_graph(drpt_ctx *c, const drpt_build_desc *desc, const void *data,
+                             int32_t *out_idx, float *out_dist, drpt_stats *stats) {
+  return build_graph_impl(c, desc, data, out_idx, out_dist, stats, nullptr);
+}
+
+static void index_free(drpt_index *x) {
+  if (!x) return;
+  cudaSetDevice(x->device);
+  void *ptrs[] = {x->X, x->order, x->goff, x->medians, x->csc_col, x->csc_row, x->csc_val,
+                  x->w1b, x->b1, x->w2, x->b2, x->c, x->inv_sigma, x->Pq, x->leaf, x->qi,
+                  x->qd, x->qx, x->qxb, x->err};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  delete x;
+}
+
+drpt_status drpt_index_build(drpt_ctx *c, const drpt_build_desc *desc, const void *data,
+                             int32_t *out_idx, float *out_dist, drpt_stats *stats,
+                             drpt_index **index) {
+  if (!c || !desc || !index) return DRPT_ERR_INVALID_ARG;
+  *index = nullptr;
+  if (desc->mode != DRPT_MODE_MIXED) {
+    set_error("an index is built by the mixed form (mode DRPT_MODE_MIXED)");
+    return DRPT_ERR_INVALID_ARG;
+  }
+  drpt_index *x = new drpt_index();
+  x->device = c->device;
+  const drpt_status st = build_graph_impl(c, desc, data, out_idx, out_dist, stats, x);
+  if (st != DRPT_OK) {
+    index_free(x);
+    return st;
+  }
+  *index = x;
+  return DRPT_OK;
+}
+
+void drpt_index_destroy(drpt_index *index) { index_free(index); }
+
+drpt_status drpt_index_query(drpt_index *x, const void *queries, int64_t nq, int32_t k,
+                             int32_t on_device, int32_t *out_idx, float *out_dist, void *stream) {
+  if (!x || !queries || !out_idx || nq <= 0 || k <= 0) return DRPT_ERR_INVALID_ARG;
+  if (k > 32) {
+    set_error("queries return at most 32 neighbours (k = %d)", k);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  DRPT_CUDA(cudaSetDevice(x->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int d = x->d, T = x->T, cols = T * (x->gd - 1);
+  const size_t esz = x->dtype == DRPT_DTYPE_U8 ? 1 : 4;
+  if (nq > x->cap) {  // grow the query scratch
+    void **bufs[] = {(void **)&x->Pq, (void **)&x->leaf, (void **)&x->qi, (void **)&x->qd,
+                     (void **)&x->qx, (void **)&x->qxb, (void **)&x->err};
+    for (void **b : bufs)
+      if (*b) {
+        cudaFree(*b);
+        *b = nullptr;
+      }
+    x->cap = 0;
+    DRPT_CUDA(cudaMalloc((void **)&x->Pq, std::max<size_t>((size_t)cols * nq, 1) * 4));
+    DRPT_CUDA(cudaMalloc((void **)&x->leaf, (size_t)T * nq * 4));
+    DRPT_CUDA(cudaMalloc((void **)&x->qi, (size_t)32 * nq * 4));
+    DRPT_CUDA(cudaMalloc((void **)&x->qd, (size_t)32 * nq * 4));
+    DRPT_CUDA(cudaMalloc(&x->qx, (size_t)nq * d * esz));
+    if (x->Tl > 0) DRPT_CUDA(cudaMalloc((void **)&x->qxb, (size_t)nq * x->d_pad * 2));
+    DRPT_CUDA(cudaMalloc((void **)&x->err, sizeof(int)));
+    x->cap = nq;
+  }
+  const void *Q = queries;
+  if (!on_device) {
+    DRPT_CUDA(cudaMemcpyAsync(x->qx, queries, (size_t)nq * d * esz, cudaMemcpyHostToDevice, s));
+    Q = x->qx;
+  }
+  // the queries' split values: random columns, then the learned MLP outputs
+  if (x->ncols_r > 0) {
+    CscDev csc{x->csc_col, x->csc_row, x->csc_val, x->ncols_r};
+    DRPT_TRY(launch_project(Q, x->dtype, nq, d, csc, x->Pq, s));
+  }
+  if (x->Tl > 0) {
+    DRPT_CUDA(cudaMemsetAsync(x->err, 0, sizeof(int), s));
+    DRPT_TRY(launch_standardise(Q, x->dtype, nq, d, x->d_pad, nullptr, x->c, x->inv_sigma, x->qxb,
+                                nullptr, s));
+    DRPT_TRY(launch_mlp_infer(x->qxb, nq, x->d_pad, x->w1b, x->Tl * (x->gd - 1), x->b1, x->w2,
+                              x->b2, x->Pq + (int64_t)x->ncols_r * nq, x->err, s));
+  }
+  DRPT_TRY(launch_descend(x->Pq, nq, T, x->gd, x->medians, x->leaf, s));
+  int32_t *oi = on_device ? out_idx : x->qi;
+  float *od = on_device ? (out_dist ? out_dist : x->qd) : x->qd;
+  DRPT_TRY(launch_query(x->X, x->dtype, d, x->n, Q, nq, T, x->order, x->goff, x->nleaf, x->leaf,
+                        k, oi, od, s));
+  if (!on_device) {
+    DRPT_CUDA(cudaMemcpyAsync(out_idx, oi, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, s));
+    if (out_dist)
+      DRPT_CUDA(cudaMemcpyAsync(out_dist, od, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, s));
+  }
+  if (x->Tl > 0) {
+    int herr = 0;
+    DRPT_CUDA(cudaMemcpyAsync(&herr, x->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    DRPT_CUDA(cudaStreamSynchronize(s));
+    if (herr) {
+      set_error("a bounded wait in the split-MLP inference kernel gave up");
+      return DRPT_ERR_TIMEOUT;
+    }
+  }
+  if (!on_device) DRPT_CUDA(cudaStreamSynchronize(s));
   return DRPT_OK;
 }
 

@@ -16,17 +16,25 @@
 // rank the reference's locality pass relabels leaves and the graph is the
 // same.
 //
-// Input formats (-data-file-format):
-//   0  IDX3 ubyte (file_reader.cpp:33-83): big-endian header magic, count,
-//      rows, cols, then count x rows x cols bytes.
+// Input formats (-data-file-format), plain or gzip-compressed:
+//   0  IDX3 ubyte (file_reader.cpp:33-83): big-endian header magic 0x803,
+//      count, rows, cols, then count x rows x cols bytes.  The magic is
+//      checked (the reference reads any header).
 //   1  raw binary (file_reader.cpp:364-497): -data-starting-index header
 //      bytes, then n x dimension values of -bytes-for-data-type bytes
 //      (4 = float32, 1 = uint8).  The values are read as stored (the
-//      reference replaces them with random draws).
+//      reference replaces them with random draws).  With the 8-byte fbin
+//      header (u32 n, u32 d) the header is checked against -dimension and
+//      -data-set-size (the reference ignores it).
 // Sizes are checked against the file; a short file is an error.
+//
+// Further flags: -precision bf16|fp8 and -learned-trees N (mixed form),
+// -write-distances 1 (a third column: the neighbour's Euclidean distance).
 
 #include <drpt_gpu.h>
+#include <zlib.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -49,6 +57,9 @@ struct Options {
   bool have_seed = false;
   uint32_t seed = 0;
   int mode = DRPT_MODE_EXACT;
+  int precision = DRPT_PRECISION_BF16;
+  int learned_trees = 0;
+  bool write_distances = false;
 };
 
 [[noreturn]] void die(const char *msg) {
@@ -86,6 +97,12 @@ Options parse(int argc, char **argv) {
     else if (!std::strcmp(f, "-leaf-size")) o.leaf_size = std::atoi(v);
     else if (!std::strcmp(f, "-tree-depth")) o.tree_depth = std::atoi(v);
     else if (!std::strcmp(f, "-device")) o.device = std::atoi(v);
+    else if (!std::strcmp(f, "-precision")) {
+      if (!std::strcmp(v, "bf16")) o.precision = DRPT_PRECISION_BF16;
+      else if (!std::strcmp(v, "fp8")) o.precision = DRPT_PRECISION_FP8_E4M3;
+      else die("-precision must be bf16 or fp8");
+    } else if (!std::strcmp(f, "-learned-trees")) o.learned_trees = std::atoi(v);
+    else if (!std::strcmp(f, "-write-distances")) o.write_distances = std::atoi(v) == 1;
   }
   // The reference's checks, in its order and with its messages (main.cpp:97-130).
   if (o.input.empty()) die("Valid input path needed!...");
@@ -101,17 +118,34 @@ uint32_t be32(const unsigned char *b) {
   return ((uint32_t)b[0] << 24) | ((uint32_t)b[1] << 16) | ((uint32_t)b[2] << 8) | b[3];
 }
 
-bool read_exact(FILE *f, void *dst, size_t bytes) { return std::fread(dst, 1, bytes, f) == bytes; }
+// gzread reads plain files unchanged, so one reader serves both.
+bool read_exact(gzFile f, void *dst, size_t bytes) {
+  unsigned char *p = static_cast<unsigned char *>(dst);
+  while (bytes > 0) {
+    const unsigned chunk = (unsigned)std::min<size_t>(bytes, 1u << 30);
+    const int got = gzread(f, p, chunk);
+    if (got <= 0) return false;
+    p += got;
+    bytes -= (size_t)got;
+  }
+  return true;
+}
+
+uint32_t le32(const unsigned char *b) {
+  return (uint32_t)b[0] | ((uint32_t)b[1] << 8) | ((uint32_t)b[2] << 16) | ((uint32_t)b[3] << 24);
+}
 
 // Returns the row-major n x d values; *dtype receives their drpt_dtype.
 std::vector<unsigned char> read_input(const Options &o, int *dtype) {
-  FILE *f = std::fopen(o.input.c_str(), "rb");
+  gzFile f = gzopen(o.input.c_str(), "rb");
   if (!f) die("cannot open the input file");
+  gzbuffer(f, 1 << 20);
   const size_t n = (size_t)o.n, d = (size_t)o.dimension;
   std::vector<unsigned char> buf;
   if (o.file_format == 0) {
     unsigned char h[16];
     if (!read_exact(f, h, 16)) die("input file shorter than an IDX3 header");
+    if (be32(h) != 0x00000803u) die("not an IDX3 ubyte file (magic is not 0x00000803)");
     const uint32_t count = be32(h + 4), rows = be32(h + 8), cols = be32(h + 12);
     if ((size_t)rows * cols != d) die("IDX3 rows x cols differs from -dimension");
     if (count < n) die("IDX3 file holds fewer images than -data-set-size");
@@ -121,8 +155,15 @@ std::vector<unsigned char> read_input(const Options &o, int *dtype) {
   } else if (o.file_format == 1) {
     if (o.bytes_for_data_type != 4 && o.bytes_for_data_type != 1)
       die("-bytes-for-data-type must be 4 (float32) or 1 (uint8)");
-    if (o.data_starting_index < 0 || std::fseek(f, o.data_starting_index, SEEK_SET) != 0)
-      die("cannot seek past the header");
+    if (o.data_starting_index < 0) die("-data-starting-index must be >= 0");
+    std::vector<unsigned char> hdr((size_t)o.data_starting_index);
+    if (!hdr.empty() && !read_exact(f, hdr.data(), hdr.size()))
+      die("input file shorter than its header");
+    if (o.data_starting_index == 8) {  // fbin: u32 n, u32 d
+      if (le32(hdr.data() + 4) != (uint32_t)o.dimension)
+        die("fbin header dimension differs from -dimension");
+      if (le32(hdr.data()) < (uint32_t)n) die("fbin header holds fewer points than -data-set-size");
+    }
     buf.resize(n * d * (size_t)o.bytes_for_data_type);
     if (!read_exact(f, buf.data(), buf.size()))
       die("binary file holds fewer than -data-set-size x -dimension values");
@@ -130,7 +171,7 @@ std::vector<unsigned char> read_input(const Options &o, int *dtype) {
   } else {
     die("Unsupported data file format, ubyte and bin file formats are supported!...");
   }
-  std::fclose(f);
+  gzclose(f);
   return buf;
 }
 
@@ -143,8 +184,8 @@ char *put_uint(char *p, uint32_t v) {
 }
 
 // Edge list: every source in ascending order, its first `per_point` entries.
-bool write_edges(const std::string &path, const std::vector<int32_t> &idx, long long n, int nn,
-                 int per_point) {
+bool write_edges(const std::string &path, const std::vector<int32_t> &idx,
+                 const std::vector<float> *dist, long long n, int nn, int per_point) {
   FILE *f = std::fopen(path.c_str(), "wb");
   if (!f) return false;
   std::vector<char> out;
@@ -153,10 +194,11 @@ bool write_edges(const std::string &path, const std::vector<int32_t> &idx, long 
     const int32_t *row = idx.data() + p * nn;
     for (int j = 0; j < per_point; ++j) {
       if (row[j] < 0) break;
-      char line[32];
+      char line[64];
       char *q = put_uint(line, (uint32_t)(p + 1));
       *q++ = ' ';
       q = put_uint(q, (uint32_t)row[j] + 1);
+      if (dist) q += std::snprintf(q, 20, " %.9g", (double)(*dist)[p * nn + j]);
       *q++ = '\n';
       out.insert(out.end(), line, q);
     }
@@ -206,10 +248,14 @@ int main(int argc, char **argv) {
   desc.local_seeds = local_seeds.data();
   desc.mode = o.mode;
   desc.leaf_size = o.leaf_size;
+  desc.precision = o.precision;
+  desc.learned_trees = o.learned_trees;
   std::vector<int32_t> idx((size_t)o.n * o.nn);
+  std::vector<float> dist(o.write_distances ? (size_t)o.n * o.nn : 0);
   drpt_stats st;
   std::memset(&st, 0, sizeof st);
-  const drpt_status rc = drpt_build_graph(ctx, &desc, data.data(), idx.data(), nullptr, &st);
+  const drpt_status rc = drpt_build_graph(ctx, &desc, data.data(), idx.data(),
+                                          o.write_distances ? dist.data() : nullptr, &st);
   if (rc != DRPT_OK) {
     std::printf("drpt: status %d: %s\n", (int)rc, drpt_last_error());
     drpt_ctx_destroy(ctx);
@@ -220,7 +266,8 @@ int main(int argc, char **argv) {
               st.global_depth, st.local_depth, seed);
 
   const auto t_w0 = clk::now();
-  if (!write_edges(o.output + "results.txt", idx, o.n, o.nn, o.nn - 1)) {
+  if (!write_edges(o.output + "results.txt", idx, o.write_distances ? &dist : nullptr, o.n, o.nn,
+                   o.nn - 1)) {
     std::printf("drpt: cannot write %sresults.txt\n", o.output.c_str());
     return 1;
   }

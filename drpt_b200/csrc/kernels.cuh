@@ -123,6 +123,13 @@ drpt_status launch_rerank(const void *X, int dtype, int d, const int32_t *visit,
                           cudaStream_t s);
 
 
+// ---- out-of-sample queries (k_query.cu) ---------------------------------------
+drpt_status launch_descend(const float *Pq, int64_t nq, int T, int gd, const float *medians,
+                           int32_t *leaf, cudaStream_t s);
+drpt_status launch_query(const void *X, int dtype, int d, int64_t n, const void *Qx, int64_t nq,
+                         int T, const int32_t *order, const int32_t *goff, int nleaf,
+                         const int32_t *leaf, int k, int32_t *oi, float *od, cudaStream_t s);
+
 // ---- learned splits (k_learned.cu) ------------------------------------------
 constexpr int kLearnHidden = 64;
 constexpr double kLearnEps = 1e-6;  // floor added to a node's variance

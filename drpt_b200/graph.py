@@ -20,8 +20,8 @@ import numpy as np
 from . import _lib
 from ._lib import DrptError, Stats, check
 
-__all__ = ["build_graph", "build_graph_batched", "MDRPT", "DrptError", "edge_list_lines",
-           "global_depth"]
+__all__ = ["build_graph", "build_graph_batched", "build_index", "Index", "MDRPT", "DrptError",
+           "edge_list_lines", "global_depth"]
 
 
 def _torch():
@@ -62,7 +62,7 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
                 tree_depth_ratio: float = 0.6, local_tree_offset: int = 2, tree_depth: int = 0,
                 density: float = 0.0, local_seeds=None, device: int = 0, stream=None,
                 out=None, leaf_size: int = 0, precision: str = "bf16", learned_trees: int = 0,
-                learn_sample: int = 0, learn_iters: int = 0):
+                learn_sample: int = 0, learn_iters: int = 0, _index_out=None):
     """k-NN graph of `data` (n x d, uint8 or float32; a NumPy array in host
     memory or a CUDA tensor).  Returns (idx, dist, stats): idx int32 and dist
     float32 of shape (n, nn), each point's nn nearest distinct neighbours other
@@ -118,9 +118,70 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
     desc.stream = stream or 0
     ctx = _lib.context(device)
     stats = Stats()
-    check(_lib.load().drpt_build_graph(ctx.handle, ctypes.byref(desc), ptr_data, ptr_idx, ptr_dist,
-                                       ctypes.byref(stats)))
+    if _index_out is not None:
+        h = ctypes.c_void_p()
+        check(_lib.load().drpt_index_build(ctx.handle, ctypes.byref(desc), ptr_data, ptr_idx,
+                                           ptr_dist, ctypes.byref(stats), ctypes.byref(h)))
+        _index_out.append(Index(h, device, desc.dtype, d, data))
+    else:
+        check(_lib.load().drpt_build_graph(ctx.handle, ctypes.byref(desc), ptr_data, ptr_idx,
+                                           ptr_dist, ctypes.byref(stats)))
     return idx, dist, stats
+
+
+class Index:
+    """Trees of a mixed-form build kept for out-of-sample queries
+    (drpt_index_build / drpt_index_query).  Holds its own device copies of
+    the rows, leaves, node medians and split functions."""
+
+    def __init__(self, handle, device: int, dtype: int, d: int, like):
+        self.handle, self.device, self.dtype, self.d = handle, device, dtype, d
+        self._cuda = _is_cuda_tensor(like)
+        self._lib = _lib.load()
+
+    def query(self, queries, k: int, stream=None):
+        """The k (<= 32) nearest indexed points of every query row among the
+        members of its leaves, by exact FP32 distance: (idx, dist) of shape
+        (nq, k), device tensors for a CUDA tensor argument, NumPy otherwise."""
+        on_dev = _is_cuda_tensor(queries)
+        q = queries.contiguous() if on_dev else np.ascontiguousarray(queries)
+        if _dtype_code(q) != self.dtype or q.shape[1] != self.d:
+            raise DrptError(1, "queries must have the index's dtype and dimension")
+        nq = int(q.shape[0])
+        if on_dev:
+            torch = _torch()
+            idx = torch.empty((nq, k), dtype=torch.int32, device=q.device)
+            dist = torch.empty((nq, k), dtype=torch.float32, device=q.device)
+            if stream is None:
+                stream = torch.cuda.current_stream(q.device).cuda_stream
+            ptrs = (q.data_ptr(), idx.data_ptr(), dist.data_ptr())
+        else:
+            idx = np.empty((nq, k), np.int32)
+            dist = np.empty((nq, k), np.float32)
+            ptrs = (q.ctypes.data, idx.ctypes.data, dist.ctypes.data)
+        check(self._lib.drpt_index_query(self.handle, ptrs[0], nq, k, 1 if on_dev else 0,
+                                         ptrs[1], ptrs[2], stream or 0))
+        return idx, dist
+
+    def close(self) -> None:
+        if self.handle:
+            self._lib.drpt_index_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def build_index(data, ntrees: int, nn: int, seed: int, **kw):
+    """build_graph in the mixed form that also returns an Index for
+    out-of-sample queries: (index, idx, dist, stats)."""
+    kw.setdefault("mode", "mixed")
+    box = []
+    idx, dist, stats = build_graph(data, ntrees, nn, seed, _index_out=box, **kw)
+    return box[0], idx, dist, stats
 
 
 def build_graph_batched(data, offsets, ntrees: int, nn: int, seed: int, *, mode: str = "mixed",

@@ -204,6 +204,26 @@ drpt_status drpt_learn_gradient(drpt_ctx *ctx, const float *Xs, int32_t S, int32
                                 const float *params, const int32_t *node, const int32_t *nbr,
                                 int32_t k, float *grad, float *loss);
 
+/* An index: a mixed-form build that keeps its trees for out-of-sample
+ * queries (no reference counterpart; the reference stores its node splits,
+ * drpt_global.cpp:290 and drpt_local.cpp:142-155, but never reads them).
+ * drpt_index_build runs drpt_build_graph (desc->mode must be
+ * DRPT_MODE_MIXED, learned trees allowed) and returns its graph and an index
+ * holding device copies of the rows, the trees' leaves and node medians and
+ * their split functions.  drpt_index_query routes each of nq query rows (d
+ * values of the index's dtype, host or device memory) down every tree by the
+ * stored medians and returns its k <= 32 nearest points among its leaves'
+ * members by exact FP32 distance, ordered by (distance, id), each point
+ * once.  The index owns its memory until drpt_index_destroy; one host thread
+ * at a time per index. */
+typedef struct drpt_index drpt_index;
+drpt_status drpt_index_build(drpt_ctx *ctx, const drpt_build_desc *desc, const void *data,
+                             int32_t *out_idx, float *out_dist, drpt_stats *stats,
+                             drpt_index **index);
+drpt_status drpt_index_query(drpt_index *index, const void *queries, int64_t nq, int32_t k,
+                             int32_t on_device, int32_t *out_idx, float *out_dist, void *stream);
+void drpt_index_destroy(drpt_index *index);
+
 /* The reference's sparse Gaussian projection matrix on the host, d x L
  * row-major, from std::mt19937(seed) (math_operations.cpp:48-76). */
 drpt_status drpt_host_projection(uint32_t seed, int32_t d, int32_t L, float density, float *B);

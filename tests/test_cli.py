@@ -1,6 +1,9 @@
 """The `drpt` command-line program: the reference CLI's flags, checks, input
 formats, edge-list file and timing line (cpp/src/main.cpp)."""
+import gzip
 import os
+import shutil
+import struct
 import subprocess
 
 import numpy as np
@@ -47,6 +50,12 @@ def test_unsupported_format_and_short_files(cli, tmp_path):
     r = _run(cli, *base, "-data-set-size", 64, "-data-file-format", 2)
     assert r.returncode == 1 and "Unsupported data file format" in r.stdout
     r = _run(cli, *base, "-data-set-size", 65, "-data-file-format", 1)
+    assert r.returncode == 1 and "fewer points" in r.stdout  # the header holds 64
+    short = tmp_path / "short.fbin"
+    with open(short, "wb") as f:  # header claims 65 points, the file holds 64
+        f.write(struct.pack("<II", 65, 16) + x.tobytes())
+    r = _run(cli, "-input", short, "-output", str(tmp_path) + "/", "-dimension", 16, "-nn", 4,
+             "-data-set-size", 65, "-data-file-format", 1)
     assert r.returncode == 1 and "fewer than" in r.stdout
     ub = tmp_path / "x.idx3"
     synth.write_idx3(str(ub), np.zeros((10, 16), np.uint8), rows=4, cols=4)
@@ -103,3 +112,57 @@ def test_cli_graph_matches_reference(cli, tmp_path, case, fmt):
     res = knn_compare.compare(ri[:, :nn - 1], rd[:, :nn - 1], got, dist[:, :nn - 1], rd)
     assert res["fail"] == 0, res
     assert os.path.getsize(out + "stats.txt") > 0
+
+
+def test_header_checks(cli, tmp_path):
+    """IDX3 magic and fbin header are checked against the flags."""
+    out = str(tmp_path) + "/"
+    bad = tmp_path / "bad.idx3"
+    with open(bad, "wb") as f:
+        f.write(struct.pack(">iiii", 0x0801, 10, 4, 4) + bytes(160))
+    r = _run(cli, "-input", bad, "-output", out, "-dimension", 16, "-nn", 4, "-data-set-size", 10)
+    assert r.returncode == 1 and "magic" in r.stdout
+    fb = tmp_path / "x.fbin"
+    synth.write_fbin(str(fb), np.zeros((64, 16), np.float32))
+    base = ["-input", fb, "-output", out, "-nn", 4, "-data-file-format", 1]
+    r = _run(cli, *base, "-dimension", 8, "-data-set-size", 64)  # 16-wide rows, 8 claimed
+    assert r.returncode == 1 and "dimension" in r.stdout
+    big = tmp_path / "big.fbin"
+    with open(big, "wb") as f:  # header says 32 points, the file holds 64
+        f.write(struct.pack("<II", 32, 16) + np.zeros((64, 16), np.float32).tobytes())
+    r = _run(cli, "-input", big, "-output", out, "-nn", 4, "-data-file-format", 1,
+             "-dimension", 16, "-data-set-size", 64)
+    assert r.returncode == 1 and "fewer points" in r.stdout
+
+
+@pytest.mark.gpu
+def test_cli_gzip_input_and_distance_column(cli, tmp_path):
+    """A gzip-compressed IDX3 file gives the same edge list as the plain one;
+    -write-distances adds each edge's FP32 distance."""
+    g = np.load(os.path.join(GOLDEN, "case_u8_c1.npz"))
+    X = g["X"]
+    n, d = X.shape
+    T, nn, seed = int(g["ntrees"]), int(g["nn"]), int(g["seeds"][0])
+    plain = tmp_path / "data.idx3"
+    synth.write_idx3(str(plain), X, rows=28, cols=28)
+    packed = tmp_path / "data.idx3.gz"
+    with open(plain, "rb") as fi, gzip.open(packed, "wb") as fo:
+        shutil.copyfileobj(fi, fo)
+    texts = []
+    for path, extra in ((plain, []), (packed, []), (packed, ["-write-distances", 1])):
+        out = tmp_path / f"o{len(texts)}"
+        out.mkdir()
+        r = _run(cli, "-input", path, "-output", str(out) + "/", "-data-set-size", n,
+                 "-dimension", d, "-ntrees", T, "-nn", nn, "-seed", seed, *extra)
+        assert r.returncode == 0, r.stdout + r.stderr
+        texts.append(open(out / "results.txt").read())
+    assert texts[0] == texts[1]
+    _, dist, _ = build_graph(X, T, nn, seed)
+    rows = [line.split() for line in texts[2].splitlines()]
+    assert [r[:2] for r in rows] == [line.split() for line in texts[0].splitlines()]
+    seen = {}
+    for src, dst, dv in rows:
+        p = int(src) - 1
+        j = seen.get(p, 0)
+        seen[p] = j + 1
+        assert float(dv) == pytest.approx(float(dist[p, j]), rel=1e-7)
