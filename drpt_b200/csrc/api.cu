@@ -400,6 +400,7 @@ drpt_status mixed_leaf_phase(drpt_ctx *c, const void *X, int dtype, int64_t n, i
   a.Xb = xb;
   DRPT_TRY(ws_get(c, "mx_nrm", (size_t)n, &a.nrm));
   DRPT_TRY(ws_get(c, "mx_scl", fp8 ? (size_t)n : 1, &a.scl));
+  DRPT_TRY(ws_get(c, "mx_mu", (size_t)nleaf * d, &a.mu));
   const size_t tiles = (size_t)ceil_div(n, 128) + nleaf;
   DRPT_TRY(ws_get(c, "mx_tile_leaf", tiles, &a.tile_leaf));
   DRPT_TRY(ws_get(c, "mx_tile_r0", tiles, &a.tile_r0));
@@ -425,7 +426,7 @@ drpt_status mixed_leaf_phase(drpt_ctx *c, const void *X, int dtype, int64_t n, i
     if (timed) DRPT_CUDA(cudaEventRecord(c->tev[3 * t + 1], s));
     DRPT_TRY(launch_leaf_mma(a, s));
     if (timed) DRPT_CUDA(cudaEventRecord(c->tev[3 * t + 2], s));
-    c->launches += 3;
+    c->launches += 4;
   }
   if (timed) DRPT_CUDA(cudaEventRecord(ev[4], s));
   // Re-rank in the leaf order of the last tree: a point's candidates are
@@ -1087,6 +1088,7 @@ drpt_status batch_prepare(drpt_ctx *c, const drpt_batch_desc *desc, const int64_
     DRPT_TRY(ws_get(c, "mx_xb", (size_t)n * d_pad * (bp->fp8 ? 1 : 2), &u8p));
     DRPT_TRY(ws_get(c, "mx_nrm", (size_t)n, &f32p));
     DRPT_TRY(ws_get(c, "mx_scl", bp->fp8 ? (size_t)n : 1, &f32p));
+    DRPT_TRY(ws_get(c, "mx_mu", (size_t)bp->nleaf * d, &f32p));
     DRPT_TRY(ws_get(c, "mx_tile_leaf", tiles, &i32p));
     DRPT_TRY(ws_get(c, "mx_tile_r0", tiles, &i32p));
     DRPT_TRY(ws_get(c, "mx_n_tiles", 1, &i32p));

@@ -5,12 +5,14 @@
 // splits) but brute-forces each whole global leaf with BF16 Gram tiles on the
 // tensor cores and wins the accuracy back afterwards:
 //
-//   K8  k_leaf_center   per global leaf: subtract the leaf mean (FP32), round
-//                       to BF16 in leaf order, row norms of the rounded rows
+//   K8  k_leaf_mean     per global leaf: the mean of its first rows
+//       k_leaf_center   per row range of a leaf: subtract the leaf mean
+//                       (FP32), round to BF16 in leaf order, row norms of the
+//                       rounded rows
 //   K9  k_tile_plan     row tiles of 128 points of every leaf
 //   K10 k_leaf_mma      per row tile: TMA-fed tcgen05 MMAs (BF16 x BF16 ->
-//                       FP32 in Tensor Memory, M = 128 rows, N = 64 columns
-//                       per tile, K = the padded dimension), epilogue scores
+//                       FP32 in Tensor Memory, M = 128 rows, N = 32 or 64
+//                       columns per tile, K = the padded dimension), epilogue scores
 //                       ||y||^2 - 2 x.y per column and keeps each row's KP
 //                       best in registers (threshold filter seeded from the
 //                       running list, per-thread shared-memory buffer,
@@ -41,15 +43,20 @@ namespace {
 using namespace sm100;
 
 constexpr int kTM = 128;            // rows per tile (M)
-constexpr int kTN = 64;             // columns per tile (N)
-// Per list width KP: B-tile stages of the resident-A pipeline, per-row
-// pending-key slots and the CTAs per SM the kernel is built for.  With 16
-// keys per row the epilogue fits 3 CTAs per SM (d <= 128: 66 KB of shared
-// memory each), so one B stage and 32 slots; with 32 keys, 2 CTAs, two
-// stages and 64 slots.
+constexpr int kTN = 64;             // columns per tile (N) of the streamed form
+// Per list width KP and A layout: columns per tile (N), accumulator buffers
+// (together 128 TMEM columns), B-tile stages, per-row pending-key slots and
+// the CTAs per SM the kernel is built for.  The epilogue bounds the kernel,
+// so the configurations maximise epilogue warps per SM: with 16 keys per row
+// and a resident A, 3 CTAs share an SM (d <= 128: 66 KB of shared memory
+// each) on one 64-column B stage and 32 slots.  (Three 32-column stages and
+// four accumulators in the same space measured slower: twice the per-tile
+// epilogue overhead.)  With 32 keys, 2 CTAs, two stages and 64 slots.
 template <int KP, bool STREAM>
 struct MmaCfg {
-  static constexpr int stages = KP == 16 ? 1 : 2;
+  static constexpr int tn = 64;
+  static constexpr int nacc = 128 / tn;
+  static constexpr int stages = (KP == 16 && !STREAM) ? 1 : 2;
   static constexpr int slots = KP == 16 ? 32 : 64;
   static constexpr int min_blocks = (KP == 16 && !STREAM) ? 3 : 2;
 };
@@ -79,14 +86,14 @@ __device__ __forceinline__ void load4<uint8_t>(const uint8_t *p, float *v) {
   v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
 }
 
-// Grid (leaves, splits): block (j, y) handles the y-th of gridDim.y row ranges
-// of global leaf j (several blocks per leaf when leaves are few).  Warps take
-// rows in turn; lane l owns the four
-// dimensions 4l..4l+3 of every 128-wide chunk (NCH chunks, d <= 128 * NCH,
-// d % 4 == 0).  The centre is the mean of the leaf's first (up to)
-// kCentreRows rows -- it only has to bring the values near zero -- summed per
-// warp, the eight warp partials added in warp order, so the result does not
-// depend on scheduling.
+// k_leaf_mean: one block per global leaf.  The centre is the mean of the
+// leaf's first (up to) kCentreRows rows -- it only has to bring the values
+// near zero -- summed per warp, the eight warp partials added in warp order,
+// so the result does not depend on scheduling.
+// k_leaf_center: grid (leaves, splits), block (j, y) handles the y-th of
+// gridDim.y row ranges of global leaf j.  Warps take rows in turn; in both
+// kernels lane l owns the four dimensions 4l..4l+3 of every 128-wide chunk
+// (NCH chunks, d <= 128 * NCH, d % 4 == 0).
 //
 // BF16 output: the centred row rounded to BF16 (d_pad elements, zero-padded).
 // E4M3 output (FP8): the centred row divided by its scale
@@ -94,47 +101,70 @@ __device__ __forceinline__ void load4<uint8_t>(const uint8_t *p, float *v) {
 // with saturation (d_pad bytes, zero-padded); the scale goes to `scl`.  In
 // both cases `nrm` receives the squared norm of the row the tensor cores see
 // (dequantised for FP8), so that ||y||^2 - 2 x.y ranks the same values.
-template <typename T, int NCH, bool FP8>
-__global__ void __launch_bounds__(256) k_leaf_center(const T *__restrict__ X, int d, int d_pad,
-                                                     const int32_t *__restrict__ order,
-                                                     const int32_t *__restrict__ goff,
-                                                     void *__restrict__ Xq,
-                                                     float *__restrict__ nrm,
-                                                     float *__restrict__ scl) {
+template <typename T, int NCH>
+__global__ void __launch_bounds__(256) k_leaf_mean(const T *__restrict__ X, int d,
+                                                   const int32_t *__restrict__ order,
+                                                   const int32_t *__restrict__ goff,
+                                                   float *__restrict__ mu) {
   constexpr int W = NCH * 128;
   __shared__ float part[8][W];
-  __shared__ float mu[W];
   const int j = blockIdx.x;
-  const int32_t lo = goff[j], hi = goff[j + 1];
-  const int m = hi - lo;
+  const int32_t lo = goff[j], m = goff[j + 1] - lo;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float acc[NCH][4];
 #pragma unroll
   for (int h = 0; h < NCH; ++h) acc[h][0] = acc[h][1] = acc[h][2] = acc[h][3] = 0.0f;
   const int mc = min(m, kCentreRows);
-  for (int r = warp; r < mc; r += 8) {
-    const T *src = X + (int64_t)__ldg(order + lo + r) * d;
+  // warp w adds rows w, w + 8, ... in order; CB rows' loads in flight at once
+  constexpr int CB = NCH <= 2 ? kCentreRows / 8 : 2;
+  for (int rb = warp; rb < mc; rb += 8 * CB) {
+    float v[CB][NCH][4];
 #pragma unroll
-    for (int h = 0; h < NCH; ++h) {
-      const int c0 = h * 128 + 4 * lane;
-      if (c0 < d) {
-        float v[4];
-        load4<T>(src + c0, v);
+    for (int i = 0; i < CB; ++i) {
+      const int r = rb + 8 * i;
+      const T *src = r < mc ? X + (int64_t)__ldg(order + lo + r) * d : nullptr;
 #pragma unroll
-        for (int e = 0; e < 4; ++e) acc[h][e] += v[e];
+      for (int h = 0; h < NCH; ++h) {
+        const int c0 = h * 128 + 4 * lane;
+        v[i][h][0] = v[i][h][1] = v[i][h][2] = v[i][h][3] = 0.0f;
+        if (src && c0 < d) load4<T>(src + c0, v[i][h]);
       }
     }
+#pragma unroll
+    for (int i = 0; i < CB; ++i)
+      if (rb + 8 * i < mc)
+#pragma unroll
+        for (int h = 0; h < NCH; ++h)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) acc[h][e] += v[i][h][e];
   }
 #pragma unroll
   for (int h = 0; h < NCH; ++h)
 #pragma unroll
     for (int e = 0; e < 4; ++e) part[warp][h * 128 + 4 * lane + e] = acc[h][e];
   __syncthreads();
-  for (int i = threadIdx.x; i < W; i += 256) {
+  for (int i = threadIdx.x; i < d; i += 256) {
     float s = 0.0f;
     for (int w = 0; w < 8; ++w) s += part[w][i];
-    mu[i] = mc > 0 ? s / (float)mc : 0.0f;
+    mu[(int64_t)j * d + i] = mc > 0 ? s / (float)mc : 0.0f;
   }
+}
+
+template <typename T, int NCH, bool FP8>
+__global__ void __launch_bounds__(256) k_leaf_center(const T *__restrict__ X, int d, int d_pad,
+                                                     const int32_t *__restrict__ order,
+                                                     const int32_t *__restrict__ goff,
+                                                     const float *__restrict__ mu_in,
+                                                     void *__restrict__ Xq,
+                                                     float *__restrict__ nrm,
+                                                     float *__restrict__ scl) {
+  constexpr int W = NCH * 128;
+  __shared__ float mu[W];
+  const int j = blockIdx.x;
+  const int32_t lo = goff[j], hi = goff[j + 1];
+  const int m = hi - lo;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = threadIdx.x; i < W; i += 256) mu[i] = i < d ? __ldg(mu_in + (int64_t)j * d + i) : 0.0f;
   __syncthreads();
   constexpr int RB = NCH <= 2 ? 4 : 1;  // rows per warp step, loaded together
   const int rb = (int)((int64_t)m * blockIdx.y / gridDim.y);
@@ -360,7 +390,7 @@ __device__ __forceinline__ void key_merge_into(float *L, const float *S) {
 // 128 E4M3 values of one 128-byte K block), 128-byte swizzled, 1024-byte
 // aligned.
 //   resident A (kb <= 2): A = kb K blocks of the 128 rows, loaded once per row
-//     tile; `stages` stages of the kb K blocks of a 64-column B tile;
+//     tile; `stages` stages of the kb K blocks of a tn-column B tile;
 //   streamed A (larger kb): kSStages stages, each one K block of A (16 KB)
 //     and of B (8 KB), so A is re-read from L2 for every column tile.
 constexpr int kSStages = 3;
@@ -370,7 +400,8 @@ struct MmaSmem {
   uint32_t a_off, b_off, buf_off, nrm_off, scl_off, bar_off, total;
 };
 
-__host__ __device__ inline MmaSmem mma_smem_layout(int kb, bool stream, int stages, int slots) {
+__host__ __device__ inline MmaSmem mma_smem_layout(int kb, bool stream, int stages, int slots,
+                                                   int tn) {
   MmaSmem L;
   L.a_off = 0;
   if (stream) {
@@ -378,12 +409,12 @@ __host__ __device__ inline MmaSmem mma_smem_layout(int kb, bool stream, int stag
     L.buf_off = kSStages * kStreamStage;
   } else {
     L.b_off = L.a_off + (uint32_t)kb * kTM * 128;
-    L.buf_off = L.b_off + (uint32_t)stages * kb * kTN * 128;
+    L.buf_off = L.b_off + (uint32_t)stages * kb * tn * 128;
   }
   L.nrm_off = L.buf_off + kTM * (uint32_t)slots * 4;
-  L.scl_off = L.nrm_off + kEpiWarps * kTN * 4;
-  L.bar_off = L.scl_off + kEpiWarps * kTN * 4;
-  L.total = L.bar_off + 16 * 8 + 16;
+  L.scl_off = L.nrm_off + kEpiWarps * (uint32_t)tn * 4;
+  L.bar_off = L.scl_off + kEpiWarps * (uint32_t)tn * 4;
+  L.total = L.bar_off + 24 * 8 + 16;
   return L;
 }
 
@@ -403,21 +434,23 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
   uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
   using Cfg = MmaCfg<KP, STREAM>;
   constexpr int kBufSlots = Cfg::slots;
-  const MmaSmem L = mma_smem_layout(kb, STREAM, Cfg::stages, Cfg::slots);
+  constexpr int TN = Cfg::tn, NACC = Cfg::nacc;
+  static_assert(!STREAM || TN == kTN, "streamed stages hold kTN-column B blocks");
+  const MmaSmem L = mma_smem_layout(kb, STREAM, Cfg::stages, Cfg::slots, TN);
   uint8_t *sA = smem + L.a_off;
   uint8_t *sB = smem + L.b_off;
   uint32_t *buf = reinterpret_cast<uint32_t *>(smem + L.buf_off);  // [slot][row] keys
-  float *nbuf = reinterpret_cast<float *>(smem + L.nrm_off);  // [warp][kTN] column norms of a tile
-  float *sbuf = reinterpret_cast<float *>(smem + L.scl_off);  // [warp][kTN] column scales (FP8)
+  float *nbuf = reinterpret_cast<float *>(smem + L.nrm_off);  // [warp][TN] column norms of a tile
+  float *sbuf = reinterpret_cast<float *>(smem + L.scl_off);  // [warp][TN] column scales (FP8)
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L.bar_off);
-  static_assert(kSStages <= 3 && Cfg::stages <= 3, "barrier slots");
+  static_assert(kSStages <= 4 && Cfg::stages <= 4 && NACC <= 4, "barrier slots");
   uint64_t *full_a = bars + 0;
-  uint64_t *full_b = bars + 1;       // up to 3 stages
-  uint64_t *empty_b = bars + 1 + 3;  // up to 3 stages
-  uint64_t *acc_full = bars + 1 + 2 * 3;
-  uint64_t *acc_empty = acc_full + 2;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 16);
-  volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 16) + 1;
+  uint64_t *full_b = bars + 1;     // up to 4 stages
+  uint64_t *empty_b = bars + 5;    // up to 4 stages
+  uint64_t *acc_full = bars + 9;   // up to 4 accumulators
+  uint64_t *acc_empty = bars + 13; // up to 4 accumulators
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 24);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 24) + 1;
   constexpr int NS = STREAM ? kSStages : Cfg::stages;
   constexpr int kKE = FP8 ? 128 : 64;  // elements per 128-byte K block
 
@@ -430,8 +463,8 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
     if (threadIdx.x == 0) atomicOr(err, 2);
     return;  // uniform for the whole block
   }
-  const int nct = (m + kTN - 1) / kTN;
-  const uint32_t a_bytes = (uint32_t)kb * kTM * 128, b_bytes = (uint32_t)kb * kTN * 128;
+  const int nct = (m + TN - 1) / TN;
+  const uint32_t a_bytes = (uint32_t)kb * kTM * 128, b_bytes = (uint32_t)kb * TN * 128;
 
   if (threadIdx.x == 0) {
     mbar_init(full_a, 1);
@@ -439,14 +472,14 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
       mbar_init(full_b + s, 1);
       mbar_init(empty_b + s, 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < NACC; ++b) {
       mbar_init(acc_full + b, 1);
       mbar_init(acc_empty + b, kEpiWarps * 32);
     }
     *abort_flag = 0;
     fence_barrier_init();
   }
-  if (warp == kEpiWarps + 1) tmem_alloc(tmem_slot, 128);  // 2 accumulators x 64 columns
+  if (warp == kEpiWarps + 1) tmem_alloc(tmem_slot, 128);  // NACC accumulators x TN columns
   if (warp == kEpiWarps && lane == 0) {
     prefetch_tmap(&tmA);
     prefetch_tmap(&tmB);
@@ -471,7 +504,7 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
           uint8_t *st = smem + (size_t)s * kStreamStage;
           mbar_arrive_expect_tx(full_b + s, kStreamStage);
           tma_load_2d(st, &tmA, full_b + s, q * kKE, lo + r0);
-          tma_load_2d(st + kStreamA, &tmB, full_b + s, q * kKE, lo + c * kTN);
+          tma_load_2d(st + kStreamA, &tmB, full_b + s, q * kKE, lo + c * TN);
         }
       } else {
         mbar_arrive_expect_tx(full_a, a_bytes);
@@ -486,7 +519,7 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
           uint8_t *dst = sB + s * b_bytes;
           mbar_arrive_expect_tx(full_b + s, b_bytes);
           for (int q = 0; q < kb; ++q)
-            tma_load_2d(dst + q * kTN * 128, &tmB, full_b + s, q * kKE, lo + c * kTN);
+            tma_load_2d(dst + q * TN * 128, &tmB, full_b + s, q * kKE, lo + c * TN);
         }
       }
     }
@@ -494,7 +527,7 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
     // ---- MMA issuer: 4 instructions per 128-byte K block (K = 16 BF16 or
     // 32 E4M3 values, 32 bytes each)
     if (lane == 0) {
-      constexpr uint32_t idesc = FP8 ? idesc_e4m3_f32(kTM, kTN) : idesc_bf16_f32(kTM, kTN);
+      constexpr uint32_t idesc = FP8 ? idesc_e4m3_f32(kTM, TN) : idesc_bf16_f32(kTM, TN);
       auto mma = [&](uint32_t d, uint64_t ad, uint64_t bd, uint32_t acc) {
         if constexpr (FP8) mma_e4m3(d, ad, bd, idesc, acc);
         else mma_bf16(d, ad, bd, idesc, acc);
@@ -502,8 +535,8 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
       bool ok = true;
       if constexpr (STREAM) {
         for (int c = 0; ok && c < nct && !*abort_flag; ++c) {
-          const int b = c & 1;
-          if (c >= 2) ok = mbar_wait(acc_empty + b, ((c >> 1) - 1) & 1);
+          const int b = c % NACC;
+          if (c >= NACC) ok = mbar_wait(acc_empty + b, ((c / NACC) - 1) & 1);
           for (int q = 0; ok && q < kb; ++q) {
             const int i = c * kb + q, s = i % NS;
             ok = mbar_wait(full_b + s, (i / NS) & 1);
@@ -512,7 +545,7 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
             const uint32_t as = smem_u32(smem + (size_t)s * kStreamStage), bs = as + kStreamA;
 #pragma unroll
             for (int k = 0; k < 4; ++k)
-              mma(tmem + b * kTN, desc_k_sw128(as + k * 32), desc_k_sw128(bs + k * 32),
+              mma(tmem + b * TN, desc_k_sw128(as + k * 32), desc_k_sw128(bs + k * 32),
                   (q | k) ? 1u : 0u);
             mma_commit(empty_b + s);
           }
@@ -522,17 +555,17 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
         const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
         ok = mbar_wait(full_a, 0);
         for (int c = 0; ok && c < nct && !*abort_flag; ++c) {
-          const int s = c % NS, b = c & 1;
+          const int s = c % NS, b = c % NACC;
           ok = mbar_wait(full_b + s, (c / NS) & 1);
-          if (ok && c >= 2) ok = mbar_wait(acc_empty + b, ((c >> 1) - 1) & 1);
+          if (ok && c >= NACC) ok = mbar_wait(acc_empty + b, ((c / NACC) - 1) & 1);
           if (!ok) break;
           tc_fence_after();
           const uint32_t bs = b_base + s * b_bytes;
           for (int q = 0; q < kb; ++q)
 #pragma unroll
             for (int k = 0; k < 4; ++k)
-              mma(tmem + b * kTN, desc_k_sw128(a_base + q * kTM * 128 + k * 32),
-                  desc_k_sw128(bs + q * kTN * 128 + k * 32), (q | k) ? 1u : 0u);
+              mma(tmem + b * TN, desc_k_sw128(a_base + q * kTM * 128 + k * 32),
+                  desc_k_sw128(bs + q * TN * 128 + k * 32), (q | k) ? 1u : 0u);
           mma_commit(empty_b + s);
           mma_commit(acc_full + b);
         }
@@ -607,8 +640,10 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
       for (int q = 0; q < kChains; ++q) aslot[q] = abase + q * kLane * kTM * 4;
       thr = fminf(thr0, td[KP - 1]);
     };
-    auto append = [&](uint32_t &slot, float sv, uint32_t col) {
-      const uint32_t key = (__float_as_uint(sv) & ~kColMask) | col;
+    // key = the score's high bits and the column bits of the packed norm
+    // (one bit-select), stored only when the score beats the threshold
+    auto append = [&](uint32_t &slot, float sv, float ncp) {
+      const uint32_t key = (__float_as_uint(sv) & ~kColMask) | (__float_as_uint(ncp) & kColMask);
       asm volatile(
           "{\n\t.reg .pred p;\n\t"
           "setp.lt.f32 p, %1, %2;\n\t"
@@ -618,42 +653,55 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
           : "f"(sv), "f"(thr), "r"(key), "n"(kTM * 4)
           : "memory");
     };
-    // one 32-column chunk of scores starting at leaf column cb
-    auto scan = [&](const float *v, const float *wn, const float *ws, uint32_t cb) {
+    // one 32-column chunk of scores; the packed norms (and E4M3 scales) of
+    // each kCheck columns are read into registers before that group's
+    // stores, so the loads do not wait behind them
+    auto scan = [&](const float *v, const float *wn, const float *ws) {
 #pragma unroll
       for (int h = 0; h < 32; h += kCheck) {
+        float nc[kCheck], sc[kCheck];
 #pragma unroll
-        for (int j4 = h; j4 < h + kCheck; j4 += 4) {
-          const float4 nc4 = *reinterpret_cast<const float4 *>(wn + j4);
-          float4 sc4 = make_float4(0.f, 0.f, 0.f, 0.f);
-          if constexpr (FP8) sc4 = *reinterpret_cast<const float4 *>(ws + j4);
-          const float scs[4] = {sc4.x, sc4.y, sc4.z, sc4.w};
-          (void)scs;
-          const float ncs[4] = {nc4.x, nc4.y, nc4.z, nc4.w};
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const int j = j4 + e;
-            float sv;
-            if constexpr (FP8) sv = fmaf(m2s * scs[e], v[j], ncs[e]);
-            else sv = fmaf(-2.0f, v[j], ncs[e]);
-            append(aslot[j % kChains], sv, cb + (uint32_t)j);
+        for (int j4 = 0; j4 < kCheck; j4 += 4) {
+          const float4 a = *reinterpret_cast<const float4 *>(wn + h + j4);
+          nc[j4] = a.x;
+          nc[j4 + 1] = a.y;
+          nc[j4 + 2] = a.z;
+          nc[j4 + 3] = a.w;
+          if constexpr (FP8) {
+            const float4 b = *reinterpret_cast<const float4 *>(ws + h + j4);
+            sc[j4] = b.x;
+            sc[j4 + 1] = b.y;
+            sc[j4 + 2] = b.z;
+            sc[j4 + 3] = b.w;
           }
+        }
+        (void)sc;
+#pragma unroll
+        for (int e = 0; e < kCheck; ++e) {
+          const int j = h + e;
+          float sv;
+          if constexpr (FP8) sv = fmaf(m2s * sc[e], v[j], nc[e]);
+          else sv = fmaf(-2.0f, v[j], nc[e]);
+          append(aslot[j % kChains], sv, nc[e]);
         }
         int most = 0;
 #pragma unroll
         for (int q = 0; q < kChains; ++q) most = max(most, pending(q));
+        // after a check that does not flush a chain holds at most
+        // kLane - kCheck / kChains keys, so the next kCheck / kChains
+        // stores stay inside its kLane slots
         if (__any_sync(kFull, most > kLane - kCheck / kChains)) flush();
       }
     };
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
     // column norms (and E4M3 scales) of a tile: lane l holds columns l and
     // l + 32, loaded one tile ahead; columns past the leaf carry an infinite
-    // norm and so never pass
-    float pn[kTN / 32], ps[kTN / 32];
+    // norm (a NaN once packed) and so never pass
+    float pn[TN / 32], ps[TN / 32];
     auto load_cols = [&](int c) {
 #pragma unroll
-      for (int h = 0; h < kTN / 32; ++h) {
-        const int col = c * kTN + h * 32 + lane;
+      for (int h = 0; h < TN / 32; ++h) {
+        const int col = c * TN + h * 32 + lane;
         const bool in = c < nct && col < m;
         pn[h] = in ? __ldg(nrm + lo + col) : __int_as_float(0x7f800000);
         ps[h] = 0.0f;
@@ -662,28 +710,33 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
     };
     load_cols(0);
     for (int c = 0; c < nct; ++c) {
-      const int b = c & 1;
+      const int b = c % NACC;
       // this tile's column norms, staged per warp (16-byte aligned reads)
-      float *wn = nbuf + warp * kTN;
-      float *ws = sbuf + warp * kTN;
+      float *wn = nbuf + warp * TN;
+      float *ws = sbuf + warp * TN;
       __syncwarp();
 #pragma unroll
-      for (int h = 0; h < kTN / 32; ++h) {
-        wn[h * 32 + lane] = pn[h];
+      for (int h = 0; h < TN / 32; ++h) {
+        // the norm's low kColBits bits replaced by the column (a relative
+        // change below 2^-10 of the norm, next to the BF16 rounding of x.y);
+        // a past-the-leaf column's infinite norm becomes a NaN, which
+        // fails every comparison
+        wn[h * 32 + lane] = __uint_as_float((__float_as_uint(pn[h]) & ~kColMask) |
+                                            (uint32_t)(c * TN + h * 32 + lane));
         if constexpr (FP8) ws[h * 32 + lane] = ps[h];
       }
       __syncwarp();
       load_cols(c + 1);
-      if (!__all_sync(kFull, mbar_wait(acc_full + b, (c >> 1) & 1))) {
+      if (!__all_sync(kFull, mbar_wait(acc_full + b, (c / NACC) & 1))) {
         *abort_flag = 1;
         break;
       }
       tc_fence_after();
 #pragma unroll
-      for (int q = 0; q < kTN / 32; ++q) {
+      for (int q = 0; q < TN / 32; ++q) {
         float v[32];
-        tmem_ld32(lane_base + b * kTN + q * 32, v);
-        scan(v, wn + q * 32, ws + q * 32, (uint32_t)(c * kTN + q * 32));
+        tmem_ld32(lane_base + b * TN + q * 32, v);
+        scan(v, wn + q * 32, ws + q * 32);
       }
       tc_fence_before();
       mbar_arrive(acc_empty + b);
@@ -748,20 +801,16 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
 }
 
 // ------------------------------------------------------------------ K11
-// One warp per point.  The warp stages the query row and its K2 candidate
-// rows in shared memory with coalesced loads (rows padded to d + 4 floats so
-// that the float4 reads below hit distinct banks), then lane j computes the
-// exact FP32 distance of candidate j: the sequential sum, in dimension order,
-// of rounded squares of rounded differences, and its rounded square root.
-// d must be a multiple of 4.
-// One warp per point.  For each candidate the warp reads the candidate row
-// with one coalesced pass (lane l holds dimensions 4l..4l+3 of every
-// 128-wide chunk), each lane adds its squared differences with fused
-// multiply-adds and a fixed butterfly adds the 32 lane sums: an FP32 distance
-// with pairwise summation, the same on every run.  Lane j then holds
-// candidate j (j < K2) and the K2 pairs are sorted with a bitonic network;
-// candidates whose distance lies within 2^-16 of the k-th are re-ordered by
-// an FP64 distance.  d must be a multiple of 4 and at most 256.
+// One warp per point.  d <= 256: four candidates at a time, eight lanes
+// each, every lane reading 16-byte pieces of the candidate row (a group reads
+// 128 contiguous bytes per load); d > 256: one candidate at a time over the
+// whole warp (lane l holds dimensions 4l..4l+3 of every 128-wide chunk).
+// Each lane adds its squared differences with fused multiply-adds and a
+// fixed butterfly adds the lane sums: an FP32 distance with pairwise
+// summation, the same on every run.  Lane j then holds candidate j (j < K2)
+// and the K2 pairs are sorted with a bitonic network; candidates whose
+// distance lies within 2^-16 of the k-th are re-ordered by an FP64
+// distance.  d must be a multiple of 4.
 template <typename T, int D, int K2>
 __global__ void __launch_bounds__(256) k_rerank(const T *__restrict__ X, int d,
                                                 const int32_t *__restrict__ visit, int64_t n,
@@ -775,38 +824,81 @@ __global__ void __launch_bounds__(256) k_rerank(const T *__restrict__ X, int d,
   const int32_t p = visit ? __ldg(visit + w) : (int32_t)w;
   const float inf = __int_as_float(0x7f800000);
   const int32_t c = lane < K2 ? __ldg(ci + (int64_t)p * K2 + lane) : -1;
-  constexpr int NC = (D + 127) / 128;  // 128-wide chunks (d <= D <= 1024)
-  float q[NC][4];
-  const T *xp = X + (int64_t)p * d;
-#pragma unroll
-  for (int h = 0; h < NC; ++h) {
-    const int c0 = h * 128 + 4 * lane;
-    q[h][0] = q[h][1] = q[h][2] = q[h][3] = 0.0f;
-    if (c0 < d) load4<T>(xp + c0, q[h]);
-  }
   float dist = inf;
-#pragma unroll 4
-  for (int jj = 0; jj < K2; ++jj) {
-    const int32_t cj = __shfl_sync(kFull, c, jj);
-    if (cj < 0) continue;  // warp-uniform
-    const T *xc = X + (int64_t)cj * d;
-    float acc = 0.0f;
+  if constexpr (D <= 256) {
+    // four candidates per pass, eight lanes each: lane s of group g holds
+    // dimensions 4s + 32t .. +3 (t < D / 32) of the query and adds the
+    // squared differences of those dimensions of candidate 4 pass + g; a
+    // fixed butterfly over the group's lanes completes the sum
+    constexpr int NQ = D / 32;
+    const int grp = lane >> 3, sl = lane & 7;
+    float q[NQ][4];
+    const T *xp = X + (int64_t)p * d;
+#pragma unroll
+    for (int t = 0; t < NQ; ++t) {
+      const int c0 = 32 * t + 4 * sl;
+      q[t][0] = q[t][1] = q[t][2] = q[t][3] = 0.0f;
+      if (c0 < d) load4<T>(xp + c0, q[t]);
+    }
+#pragma unroll
+    for (int pass = 0; pass < K2 / 4; ++pass) {
+      const int32_t cj = __shfl_sync(kFull, c, 4 * pass + grp);
+      float acc = 0.0f;
+      if (cj >= 0) {
+        const T *xc = X + (int64_t)cj * d;
+#pragma unroll
+        for (int t = 0; t < NQ; ++t) {
+          const int c0 = 32 * t + 4 * sl;
+          if (c0 < d) {
+            float v[4];
+            load4<T>(xc + c0, v);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const float df = v[e] - q[t][e];
+              acc = fmaf(df, df, acc);
+            }
+          }
+        }
+      }
+      acc += __shfl_xor_sync(kFull, acc, 4);
+      acc += __shfl_xor_sync(kFull, acc, 2);
+      acc += __shfl_xor_sync(kFull, acc, 1);
+      const float got = __shfl_sync(kFull, acc, 8 * (lane & 3));
+      if ((lane >> 2) == pass && c >= 0) dist = sqrtf(got);
+    }
+  } else {
+    constexpr int NC = (D + 127) / 128;  // 128-wide chunks (d <= D <= 1024)
+    float q[NC][4];
+    const T *xp = X + (int64_t)p * d;
 #pragma unroll
     for (int h = 0; h < NC; ++h) {
       const int c0 = h * 128 + 4 * lane;
-      if (c0 < d) {
-        float v[4];
-        load4<T>(xc + c0, v);
+      q[h][0] = q[h][1] = q[h][2] = q[h][3] = 0.0f;
+      if (c0 < d) load4<T>(xp + c0, q[h]);
+    }
+#pragma unroll 4
+    for (int jj = 0; jj < K2; ++jj) {
+      const int32_t cj = __shfl_sync(kFull, c, jj);
+      if (cj < 0) continue;  // warp-uniform
+      const T *xc = X + (int64_t)cj * d;
+      float acc = 0.0f;
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const float df = v[e] - q[h][e];
-          acc = fmaf(df, df, acc);
+      for (int h = 0; h < NC; ++h) {
+        const int c0 = h * 128 + 4 * lane;
+        if (c0 < d) {
+          float v[4];
+          load4<T>(xc + c0, v);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const float df = v[e] - q[h][e];
+            acc = fmaf(df, df, acc);
+          }
         }
       }
-    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
-    if (lane == jj) dist = sqrtf(acc);
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+      if (lane == jj) dist = sqrtf(acc);
+    }
   }
   int32_t id = c;
   // bitonic sort of K2 (dist, id) pairs inside the group, ascending
@@ -941,17 +1033,19 @@ drpt_status make_tmap(CUtensorMap *map, const void *base, int64_t rows, int d_pa
 
 template <typename T, int NCH>
 void center_t(const MixedTreeArgs &a, cudaStream_t s) {
-  // enough blocks for about four per SM, at least 64 rows per block
+  // about 128 rows per block (at most 64 blocks per leaf), so that uneven
+  // leaf sizes do not leave a tail of long blocks
   const int64_t mean = a.n / a.nleaf;
-  const int64_t split = std::max<int64_t>(
-      1, std::min<int64_t>(ceil_div(4 * 148, a.nleaf), mean / 64));
+  const int64_t split = std::max<int64_t>(1, std::min<int64_t>(64, mean / 128));
   const dim3 grid((unsigned)a.nleaf, (unsigned)split);
+  k_leaf_mean<T, NCH><<<(unsigned)a.nleaf, 256, 0, s>>>((const T *)a.X, a.d, a.order, a.goff,
+                                                       a.mu);
   if (a.fp8)
     k_leaf_center<T, NCH, true><<<grid, 256, 0, s>>>((const T *)a.X, a.d, a.d_pad, a.order,
-                                                     a.goff, a.Xb, a.nrm, a.scl);
+                                                     a.goff, a.mu, a.Xb, a.nrm, a.scl);
   else
     k_leaf_center<T, NCH, false><<<grid, 256, 0, s>>>((const T *)a.X, a.d, a.d_pad, a.order,
-                                                      a.goff, a.Xb, a.nrm, a.scl);
+                                                      a.goff, a.mu, a.Xb, a.nrm, a.scl);
 }
 
 template <typename T>
@@ -962,10 +1056,11 @@ void center_d(const MixedTreeArgs &a, cudaStream_t s) {
 }
 
 template <int KP, bool STREAM, bool FP8>
-drpt_status mma_t(const MixedTreeArgs &a, const CUtensorMap &tmA, const CUtensorMap &tmB, int kb,
-                  cudaStream_t s) {
-  const MmaSmem L = mma_smem_layout(kb, STREAM, MmaCfg<KP, STREAM>::stages,
-                                    MmaCfg<KP, STREAM>::slots);
+drpt_status mma_t(const MixedTreeArgs &a, const CUtensorMap &tmA, int kb, cudaStream_t s) {
+  using Cfg = MmaCfg<KP, STREAM>;
+  CUtensorMap tmB;
+  DRPT_TRY(make_tmap(&tmB, a.Xb, a.n, a.d_pad, Cfg::tn, a.fp8));
+  const MmaSmem L = mma_smem_layout(kb, STREAM, Cfg::stages, Cfg::slots, Cfg::tn);
   const size_t smem = L.total + 1024;
   if (smem > 227 * 1024) {
     set_error("mixed leaf kernel: %zu bytes of shared memory needed", smem);
@@ -982,14 +1077,13 @@ drpt_status mma_t(const MixedTreeArgs &a, const CUtensorMap &tmA, const CUtensor
 }
 
 template <int KP>
-drpt_status mma_kp(const MixedTreeArgs &a, const CUtensorMap &tmA, const CUtensorMap &tmB, int kb,
-                   cudaStream_t s) {
+drpt_status mma_kp(const MixedTreeArgs &a, const CUtensorMap &tmA, int kb, cudaStream_t s) {
   // Resident A only for up to two K blocks: beyond that the streamed
   // stages fit two CTAs per SM where a resident A tile fits one.
   const bool stream = kb > 2;
   if (a.fp8)
-    return stream ? mma_t<KP, true, true>(a, tmA, tmB, kb, s) : mma_t<KP, false, true>(a, tmA, tmB, kb, s);
-  return stream ? mma_t<KP, true, false>(a, tmA, tmB, kb, s) : mma_t<KP, false, false>(a, tmA, tmB, kb, s);
+    return stream ? mma_t<KP, true, true>(a, tmA, kb, s) : mma_t<KP, false, true>(a, tmA, kb, s);
+  return stream ? mma_t<KP, true, false>(a, tmA, kb, s) : mma_t<KP, false, false>(a, tmA, kb, s);
 }
 
 }  // namespace
@@ -1017,12 +1111,11 @@ drpt_status launch_leaf_mma(const MixedTreeArgs &a, cudaStream_t s) {
   }
   k_tile_plan<<<1, 1024, 0, s>>>(a.goff, a.nleaf, a.tile_leaf, a.tile_r0, a.n_tiles);
   DRPT_LAUNCH_CHECK();
-  CUtensorMap tmA, tmB;
+  CUtensorMap tmA;
   DRPT_TRY(make_tmap(&tmA, a.Xb, a.n, a.d_pad, kTM, a.fp8));
-  DRPT_TRY(make_tmap(&tmB, a.Xb, a.n, a.d_pad, kTN, a.fp8));
   const int kb = a.d_pad * esz / 128;
-  if (a.kp == 16) return mma_kp<16>(a, tmA, tmB, kb, s);
-  if (a.kp == 32) return mma_kp<32>(a, tmA, tmB, kb, s);
+  if (a.kp == 16) return mma_kp<16>(a, tmA, kb, s);
+  if (a.kp == 32) return mma_kp<32>(a, tmA, kb, s);
   set_error("mixed leaf kernel: %d candidates per tree unsupported (16 or 32)", a.kp);
   return DRPT_ERR_UNSUPPORTED;
 }

@@ -28,12 +28,17 @@ __device__ __forceinline__ float4 load4v(const uint8_t *p) {
 }
 
 // Block: `pts` consecutive points (or the block table's entry: first point,
-// points, column set); thread pairs (point, column) with the point index
-// fastest so a warp writes 32 consecutive P entries of a column.
-template <typename T>
+// points, column set).  The rows are staged as floats with a row stride of
+// d + 1 (odd for even d, so 32 lanes reading one dimension of 32 rows hit 32
+// banks).  Staging: the block's rows are one contiguous range of d / 4 quads
+// per row; thread t takes quads t, t + 256, ..., eight loads in flight
+// before their stores.  Products: warp w takes output columns w, w + 8, ...;
+// lane l the points l + 32 i (i < PPL, PPL * 32 >= points), PPL independent
+// sums that share each nonzero of the column.
+template <typename T, int PPL>
 __global__ void __launch_bounds__(kThreads) k_project(const T *__restrict__ X, int64_t n, int d,
                                                       CscDev csc, float *__restrict__ P, int pts) {
-  extern __shared__ float xs[];  // pts x (d + 1), padded against bank conflicts
+  extern __shared__ float xs[];  // pts x (d + 1)
   int64_t p0 = (int64_t)blockIdx.x * pts;
   int np = (int)min64(pts, n - p0);
   if (csc.blocks) {
@@ -42,22 +47,40 @@ __global__ void __launch_bounds__(kThreads) k_project(const T *__restrict__ X, i
     np = b[1];
     csc.colptr += (int64_t)b[2] * (csc.ncols + 1);
   }
+  if (np <= 0) return;  // uniform for the whole block
   const int ld = d + 1;
   const T *src = X + p0 * d;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (d % 4 == 0) {
-    // Stage the rows with 4-element loads: warp w takes rows w, w + 8, ...,
-    // lane l the quads l, l + 32, ... of a row (no index division).
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, q4 = d >> 2;
-#pragma unroll 2
-    for (int r = warp; r < np; r += kThreads / 32) {
-      const T *row = src + (int64_t)r * d;
-      float *dst = xs + r * ld;
-      for (int c4 = lane; c4 < q4; c4 += 32) {
-        const float4 v = load4v(row + 4 * c4);
-        dst[4 * c4] = v.x;
-        dst[4 * c4 + 1] = v.y;
-        dst[4 * c4 + 2] = v.z;
-        dst[4 * c4 + 3] = v.w;
+    constexpr int kBatch = 8;
+    const int q4 = d >> 2, total = np * q4;
+    // quad qi = r * q4 + c4, walked in steps of kThreads without division
+    int r = threadIdx.x / q4, c4 = threadIdx.x - r * q4;
+    const int dr = kThreads / q4, dc = kThreads - dr * q4;
+    for (int qb = threadIdx.x; qb < total; qb += kBatch * kThreads) {
+      float4 v[kBatch];
+      int rr[kBatch], cc[kBatch];
+#pragma unroll
+      for (int i = 0; i < kBatch; ++i) {
+        rr[i] = r;
+        cc[i] = c4;
+        if (qb + i * kThreads < total) v[i] = load4v(src + (int64_t)r * d + 4 * c4);
+        r += dr;
+        c4 += dc;
+        if (c4 >= q4) {
+          c4 -= q4;
+          ++r;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < kBatch; ++i) {
+        if (qb + i * kThreads < total) {
+          float *dst = xs + rr[i] * ld + 4 * cc[i];
+          dst[0] = v[i].x;
+          dst[1] = v[i].y;
+          dst[2] = v[i].z;
+          dst[3] = v[i].w;
+        }
       }
     }
   } else {
@@ -69,21 +92,38 @@ __global__ void __launch_bounds__(kThreads) k_project(const T *__restrict__ X, i
     }
   }
   __syncthreads();
-  // pairs q = col * np + r, walked in steps of the block size without division
-  const int pairs = np * csc.ncols;
-  int col = threadIdx.x / np, r = threadIdx.x - col * np;
-  for (int q = threadIdx.x; q < pairs; q += kThreads) {
+  // rows past the block's points read its last row and are not written
+  int off[PPL];
+#pragma unroll
+  for (int i = 0; i < PPL; ++i) off[i] = min(lane + 32 * i, np - 1) * ld;
+  for (int col = warp; col < csc.ncols; col += kThreads / 32) {
     const int e0 = __ldg(csc.colptr + col), e1 = __ldg(csc.colptr + col + 1);
-    const float *x = xs + r * ld;
-    float acc = 0.0f;
-    for (int e = e0; e < e1; ++e) acc = __fadd_rn(acc, __fmul_rn(x[__ldg(csc.row + e)], __ldg(csc.val + e)));
-    P[(int64_t)col * n + p0 + r] = acc;
-    r += kThreads;
-    while (r >= np) {
-      r -= np;
-      ++col;
+    float acc[PPL];
+#pragma unroll
+    for (int i = 0; i < PPL; ++i) acc[i] = 0.0f;
+    for (int e = e0; e < e1; ++e) {
+      const int k = __ldg(csc.row + e);
+      const float b = __ldg(csc.val + e);
+#pragma unroll
+      for (int i = 0; i < PPL; ++i) acc[i] = __fadd_rn(acc[i], __fmul_rn(xs[off[i] + k], b));
     }
+    float *out = P + (int64_t)col * n + p0;
+#pragma unroll
+    for (int i = 0; i < PPL; ++i)
+      if (lane + 32 * i < np) out[lane + 32 * i] = acc[i];
   }
+}
+
+template <typename T>
+void project_t(const void *X, int64_t n, int d, const CscDev &csc, float *P, int pts,
+               unsigned grid, size_t smem, cudaStream_t s) {
+  auto launch = [&](auto kern) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern<<<grid, kThreads, smem, s>>>((const T *)X, n, d, csc, P, pts);
+  };
+  if (pts <= 32) launch(k_project<T, 1>);
+  else if (pts <= 64) launch(k_project<T, 2>);
+  else launch(k_project<T, 4>);
 }
 
 }  // namespace
@@ -104,15 +144,8 @@ drpt_status launch_project(const void *X, int dtype, int64_t n, int d, const Csc
     return DRPT_ERR_UNSUPPORTED;
   }
   const unsigned grid = csc.blocks ? (unsigned)csc.nblocks : (unsigned)ceil_div(n, pts);
-  if (dtype == DRPT_DTYPE_U8) {
-    DRPT_CUDA(cudaFuncSetAttribute(k_project<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
-    k_project<uint8_t><<<grid, kThreads, smem, s>>>((const uint8_t *)X, n, d, csc, P, pts);
-  } else {
-    DRPT_CUDA(cudaFuncSetAttribute(k_project<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
-    k_project<float><<<grid, kThreads, smem, s>>>((const float *)X, n, d, csc, P, pts);
-  }
+  if (dtype == DRPT_DTYPE_U8) project_t<uint8_t>(X, n, d, csc, P, pts, grid, smem, s);
+  else project_t<float>(X, n, d, csc, P, pts, grid, smem, s);
   DRPT_LAUNCH_CHECK();
   return DRPT_OK;
 }

@@ -106,6 +106,7 @@ struct MixedTreeArgs {
   void *Xb;                  // n x d_pad centred rows in leaf order (BF16 or E4M3)
   float *nrm;                // n, squared norms of the rows the tensor cores see
   float *scl;                // n, per-row E4M3 scales (FP8 only)
+  float *mu;                 // nleaf x d, leaf centres
   int32_t *tile_leaf, *tile_r0, *n_tiles;  // n / 128 + nleaf
   int32_t *cand_idx;         // n x kp running list (point ids), updated tree by tree
   float *cand_dist;          // n x kp approximate squared distances, ascending
