@@ -34,7 +34,9 @@ struct drpt_ctx {
   std::map<std::string, Buf> bufs;
   std::map<std::pair<int64_t, int>, std::pair<std::vector<int32_t>, std::vector<int32_t>>> perms;
   cudaEvent_t ev[8] = {};
-  std::vector<cudaEvent_t> tev;  // per-tree event pairs (mixed mode)
+  std::vector<cudaEvent_t> tev;  // event pool of the mixed form's leaf phase
+  // (start, end) indices into tev of its staging and tensor-core spans
+  std::vector<std::pair<int, int>> tstage, tmma;
   int launches = 0;
   uint64_t ws_gen = 0;           // bumped whenever a workspace buffer moves
   // batches: the captured device work of the last graph-mode batch
@@ -395,12 +397,30 @@ drpt_status mixed_leaf_phase(drpt_ctx *c, const void *X, int dtype, int64_t n, i
   a.T = T;
   a.kp = kp;
   a.fp8 = fp8;
+  const int Tc = mixed_stage_trees(n, d_pad, fp8, T);
+  const size_t row_bytes = (size_t)d_pad * (fp8 ? 1 : 2);
   uint8_t *xb = nullptr;
-  DRPT_TRY(ws_get(c, "mx_xb", (size_t)n * d_pad * (fp8 ? 1 : 2), &xb));
-  a.Xb = xb;
-  DRPT_TRY(ws_get(c, "mx_nrm", (size_t)n, &a.nrm));
-  DRPT_TRY(ws_get(c, "mx_scl", fp8 ? (size_t)n : 1, &a.scl));
-  DRPT_TRY(ws_get(c, "mx_mu", (size_t)nleaf * d, &a.mu));
+  float *nrm = nullptr, *scl = nullptr;
+  DRPT_TRY(ws_get(c, "mx_xb", (size_t)Tc * n * row_bytes, &xb));
+  DRPT_TRY(ws_get(c, "mx_nrm", (size_t)Tc * n, &nrm));
+  DRPT_TRY(ws_get(c, "mx_scl", fp8 ? (size_t)Tc * n : 1, &scl));
+  LeafStageArgs st{};
+  st.X = X;
+  st.dtype = dtype;
+  st.n = n;
+  st.d = d;
+  st.d_pad = d_pad;
+  st.fp8 = fp8;
+  st.order = order;
+  st.goff = goff;
+  st.nleaf = nleaf;
+  st.T = T;
+  DRPT_TRY(ws_get(c, "mx_pos", (size_t)T * n, &st.pos));
+  DRPT_TRY(ws_get(c, "mx_lf", (size_t)T * n, &st.lf));
+  DRPT_TRY(ws_get(c, "mx_mu", (size_t)T * nleaf * d, &st.mu));
+  st.Xb = xb;
+  st.nrm = nrm;
+  st.scl = scl;
   const size_t tiles = (size_t)ceil_div(n, 128) + nleaf;
   DRPT_TRY(ws_get(c, "mx_tile_leaf", tiles, &a.tile_leaf));
   DRPT_TRY(ws_get(c, "mx_tile_r0", tiles, &a.tile_r0));
@@ -409,24 +429,56 @@ drpt_status mixed_leaf_phase(drpt_ctx *c, const void *X, int dtype, int64_t n, i
   DRPT_TRY(ws_get(c, "mx_run_idx", (size_t)n * kp, &a.cand_idx));
   DRPT_TRY(ws_get(c, "mx_run_dist", (size_t)n * kp, &a.cand_dist));
   DRPT_CUDA(cudaMemsetAsync(a.err, 0, sizeof(int), s));
+  int nev = 0;
   if (timed) {
     DRPT_CUDA(cudaEventRecord(ev[3], s));
-    while ((int)c->tev.size() < 3 * T) {
+    const int need = 2 + 2 * T + 2 * T;
+    while ((int)c->tev.size() < need) {
       cudaEvent_t e;
       DRPT_CUDA(cudaEventCreate(&e));
       c->tev.push_back(e);
     }
+    c->tstage.clear();
+    c->tmma.clear();
   }
-  for (int t = 0; t < T; ++t) {
-    a.tree = t;
-    a.order = order + (size_t)t * n;
-    a.goff = goff + (size_t)t * (nleaf + 1);
-    if (timed) DRPT_CUDA(cudaEventRecord(c->tev[3 * t], s));
-    DRPT_TRY(launch_leaf_center(a, s));
-    if (timed) DRPT_CUDA(cudaEventRecord(c->tev[3 * t + 1], s));
-    DRPT_TRY(launch_leaf_mma(a, s));
-    if (timed) DRPT_CUDA(cudaEventRecord(c->tev[3 * t + 2], s));
-    c->launches += 4;
+  auto mark = [&](int *idx) -> drpt_status {
+    *idx = nev++;
+    DRPT_CUDA(cudaEventRecord(c->tev[*idx], s));
+    return DRPT_OK;
+  };
+  int e0 = 0, e1 = 0;
+  if (timed) DRPT_TRY(mark(&e0));
+  DRPT_TRY(launch_leaf_means(st, s));
+  c->launches += 2;
+  if (timed) {
+    DRPT_TRY(mark(&e1));
+    c->tstage.push_back({e0, e1});
+  }
+  for (int t0 = 0; t0 < T; t0 += Tc) {
+    st.t0 = t0;
+    st.tc = std::min(Tc, T - t0);
+    if (timed) DRPT_TRY(mark(&e0));
+    DRPT_TRY(launch_leaf_stage(st, s));
+    c->launches += 1;
+    if (timed) {
+      DRPT_TRY(mark(&e1));
+      c->tstage.push_back({e0, e1});
+    }
+    for (int t = t0; t < t0 + st.tc; ++t) {
+      a.tree = t;
+      a.order = order + (size_t)t * n;
+      a.goff = goff + (size_t)t * (nleaf + 1);
+      a.Xb = xb + (size_t)(t - t0) * n * row_bytes;
+      a.nrm = nrm + (size_t)(t - t0) * n;
+      a.scl = fp8 ? scl + (size_t)(t - t0) * n : scl;
+      if (timed) DRPT_TRY(mark(&e0));
+      DRPT_TRY(launch_leaf_mma(a, s));
+      c->launches += 2;
+      if (timed) {
+        DRPT_TRY(mark(&e1));
+        c->tmma.push_back({e0, e1});
+      }
+    }
   }
   if (timed) DRPT_CUDA(cudaEventRecord(ev[4], s));
   // Re-rank in the leaf order of the last tree: a point's candidates are
@@ -436,6 +488,12 @@ drpt_status mixed_leaf_phase(drpt_ctx *c, const void *X, int dtype, int64_t n, i
   c->launches += 1;
   if (timed) DRPT_CUDA(cudaEventRecord(ev[5], s));
   return DRPT_OK;
+}
+
+// Staging and tensor-core milliseconds of the last timed leaf phase.
+void leaf_phase_ms(drpt_ctx *c, float *stage, float *mma) {
+  for (const auto &p : c->tstage) *stage += elapsed(c->tev[p.first], c->tev[p.second]);
+  for (const auto &p : c->tmma) *mma += elapsed(c->tev[p.first], c->tev[p.second]);
 }
 
 drpt_status mixed_check(drpt_ctx *c, cudaStream_t s) {
@@ -860,10 +918,7 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
         padded += ceil_div(m, 128) * 128 * ceil_div(m, 64) * 64;
       }
     stats->mma_pairs_padded = padded;
-    for (int t = 0; t < T; ++t) {
-      stats->ms_leaf_stage += elapsed(c->tev[3 * t], c->tev[3 * t + 1]);
-      stats->ms_leaf_mma += elapsed(c->tev[3 * t + 1], c->tev[3 * t + 2]);
-    }
+    leaf_phase_ms(c, &stats->ms_leaf_stage, &stats->ms_leaf_mma);
     stats->min_global_leaf = mn;
     stats->max_final_leaf = mx;
     stats->kernels_launched = c->launches - launches0;
@@ -1085,10 +1140,13 @@ drpt_status batch_prepare(drpt_ctx *c, const drpt_batch_desc *desc, const int64_
     int32_t *i32p;
     float *f32p;
     int *ip;
-    DRPT_TRY(ws_get(c, "mx_xb", (size_t)n * d_pad * (bp->fp8 ? 1 : 2), &u8p));
-    DRPT_TRY(ws_get(c, "mx_nrm", (size_t)n, &f32p));
-    DRPT_TRY(ws_get(c, "mx_scl", bp->fp8 ? (size_t)n : 1, &f32p));
-    DRPT_TRY(ws_get(c, "mx_mu", (size_t)bp->nleaf * d, &f32p));
+    const int Tc = mixed_stage_trees(n, d_pad, bp->fp8, T);
+    DRPT_TRY(ws_get(c, "mx_xb", (size_t)Tc * n * d_pad * (bp->fp8 ? 1 : 2), &u8p));
+    DRPT_TRY(ws_get(c, "mx_nrm", (size_t)Tc * n, &f32p));
+    DRPT_TRY(ws_get(c, "mx_scl", bp->fp8 ? (size_t)Tc * n : 1, &f32p));
+    DRPT_TRY(ws_get(c, "mx_pos", (size_t)T * n, &i32p));
+    DRPT_TRY(ws_get(c, "mx_lf", (size_t)T * n, &i32p));
+    DRPT_TRY(ws_get(c, "mx_mu", (size_t)T * bp->nleaf * d, &f32p));
     DRPT_TRY(ws_get(c, "mx_tile_leaf", tiles, &i32p));
     DRPT_TRY(ws_get(c, "mx_tile_r0", tiles, &i32p));
     DRPT_TRY(ws_get(c, "mx_n_tiles", 1, &i32p));
@@ -1343,11 +1401,7 @@ drpt_status drpt_build_graph_batched(drpt_ctx *c, const drpt_batch_desc *desc,
     stats->ms_leaf_knn = elapsed(ev[3], ev[4]);
     stats->ms_merge = elapsed(ev[4], ev[5]);
     stats->ms_total = elapsed(ev[0], ev[6]);
-    if (desc->mode == DRPT_MODE_MIXED)
-      for (int t = 0; t < bp.T; ++t) {
-        stats->ms_leaf_stage += elapsed(c->tev[3 * t], c->tev[3 * t + 1]);
-        stats->ms_leaf_mma += elapsed(c->tev[3 * t + 1], c->tev[3 * t + 2]);
-      }
+    if (desc->mode == DRPT_MODE_MIXED) leaf_phase_ms(c, &stats->ms_leaf_stage, &stats->ms_leaf_mma);
   }
   if (desc->use_graph) {
     // capture the device work of this batch for the next calls (every

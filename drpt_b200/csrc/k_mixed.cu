@@ -5,10 +5,13 @@
 // splits) but brute-forces each whole global leaf with BF16 Gram tiles on the
 // tensor cores and wins the accuracy back afterwards:
 //
-//   K8  k_leaf_mean     per global leaf: the mean of its first rows
-//       k_leaf_center   per row range of a leaf: subtract the leaf mean
-//                       (FP32), round to BF16 in leaf order, row norms of the
-//                       rounded rows
+//   K8  k_leaf_index    per tree and point: its row in the tree's leaf order
+//                       and its leaf
+//       k_leaf_mean     per tree and global leaf: the mean of its first rows
+//       k_leaf_stage    per point, read once in index order, for every tree of
+//                       a chunk: subtract its leaf's mean (FP32), round to
+//                       BF16, store at its row in that tree's leaf order, norm
+//                       of the rounded row
 //   K9  k_tile_plan     row tiles of 128 points of every leaf
 //   K10 k_leaf_mma      per row tile: TMA-fed tcgen05 MMAs (BF16 x BF16 ->
 //                       FP32 in Tensor Memory, M = 128 rows, N = 32 or 64
@@ -86,30 +89,55 @@ __device__ __forceinline__ void load4<uint8_t>(const uint8_t *p, float *v) {
   v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
 }
 
-// k_leaf_mean: one block per global leaf.  The centre is the mean of the
-// leaf's first (up to) kCentreRows rows -- it only has to bring the values
-// near zero -- summed per warp, the eight warp partials added in warp order,
-// so the result does not depend on scheduling.
-// k_leaf_center: grid (leaves, splits), block (j, y) handles the y-th of
-// gridDim.y row ranges of global leaf j.  Warps take rows in turn; in both
-// kernels lane l owns the four dimensions 4l..4l+3 of every 128-wide chunk
-// (NCH chunks, d <= 128 * NCH, d % 4 == 0).
-//
-// BF16 output: the centred row rounded to BF16 (d_pad elements, zero-padded).
-// E4M3 output (FP8): the centred row divided by its scale
-// s = max|x - c| / 448 (448 = largest finite E4M3 value) and rounded to E4M3
-// with saturation (d_pad bytes, zero-padded); the scale goes to `scl`.  In
-// both cases `nrm` receives the squared norm of the row the tensor cores see
-// (dequantised for FP8), so that ||y||^2 - 2 x.y ranks the same values.
+// Streaming variants for data read or written once (evict-first in L2, so
+// that the leaf centres stay resident).
+template <typename T>
+__device__ __forceinline__ void load4_cs(const T *p, float *v);
+template <>
+__device__ __forceinline__ void load4_cs<float>(const float *p, float *v) {
+  const float4 q = __ldcs(reinterpret_cast<const float4 *>(p));
+  v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+template <>
+__device__ __forceinline__ void load4_cs<uint8_t>(const uint8_t *p, float *v) {
+  const uchar4 q = __ldcs(reinterpret_cast<const uchar4 *>(p));
+  v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+
+// k_leaf_index: block (j, t) writes, for every point of leaf j of tree t,
+// its position in the tree's leaf order and the leaf.
+__global__ void __launch_bounds__(256) k_leaf_index(const int32_t *__restrict__ order,
+                                                    const int32_t *__restrict__ goff, int64_t n,
+                                                    int nleaf, int32_t *__restrict__ pos,
+                                                    int32_t *__restrict__ lf) {
+  const int j = blockIdx.x, t = blockIdx.y;
+  const int32_t *o = order + (int64_t)t * n;
+  const int32_t *g = goff + (int64_t)t * (nleaf + 1);
+  const int32_t lo = g[j], hi = g[j + 1];
+  for (int32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const int32_t p = __ldg(o + i);
+    pos[(int64_t)t * n + p] = i;
+    lf[(int64_t)t * n + p] = j;
+  }
+}
+
+// k_leaf_mean: block (j, t) for leaf j of tree t.  The centre is the mean of
+// the leaf's first (up to) kCentreRows rows -- it only has to bring the
+// values near zero -- summed per warp, the eight warp partials added in warp
+// order, so the result does not depend on scheduling.  In both this kernel
+// and k_leaf_stage lane l owns the four dimensions 4l..4l+3 of every 128-wide
+// chunk (NCH chunks, d <= 128 * NCH, d % 4 == 0).
 template <typename T, int NCH>
-__global__ void __launch_bounds__(256) k_leaf_mean(const T *__restrict__ X, int d,
+__global__ void __launch_bounds__(256) k_leaf_mean(const T *__restrict__ X, int64_t n, int d,
                                                    const int32_t *__restrict__ order,
-                                                   const int32_t *__restrict__ goff,
+                                                   const int32_t *__restrict__ goff, int nleaf,
                                                    float *__restrict__ mu) {
   constexpr int W = NCH * 128;
   __shared__ float part[8][W];
-  const int j = blockIdx.x;
-  const int32_t lo = goff[j], m = goff[j + 1] - lo;
+  const int j = blockIdx.x, t = blockIdx.y;
+  const int32_t *ord = order + (int64_t)t * n;
+  const int32_t *g = goff + (int64_t)t * (nleaf + 1);
+  const int32_t lo = g[j], m = g[j + 1] - lo;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float acc[NCH][4];
 #pragma unroll
@@ -122,7 +150,7 @@ __global__ void __launch_bounds__(256) k_leaf_mean(const T *__restrict__ X, int 
 #pragma unroll
     for (int i = 0; i < CB; ++i) {
       const int r = rb + 8 * i;
-      const T *src = r < mc ? X + (int64_t)__ldg(order + lo + r) * d : nullptr;
+      const T *src = r < mc ? X + (int64_t)__ldg(ord + lo + r) * d : nullptr;
 #pragma unroll
       for (int h = 0; h < NCH; ++h) {
         const int c0 = h * 128 + 4 * lane;
@@ -143,112 +171,155 @@ __global__ void __launch_bounds__(256) k_leaf_mean(const T *__restrict__ X, int 
 #pragma unroll
     for (int e = 0; e < 4; ++e) part[warp][h * 128 + 4 * lane + e] = acc[h][e];
   __syncthreads();
+  float *out = mu + ((int64_t)t * nleaf + j) * d;
   for (int i = threadIdx.x; i < d; i += 256) {
     float s = 0.0f;
     for (int w = 0; w < 8; ++w) s += part[w][i];
-    mu[(int64_t)j * d + i] = mc > 0 ? s / (float)mc : 0.0f;
+    out[i] = mc > 0 ? s / (float)mc : 0.0f;
   }
 }
 
+// k_leaf_stage: warps take RB consecutive points at a time (grid-stride) and
+// read their rows once; for every tree t of the chunk each point's row is
+// centred on its leaf's mean and stored at its position in tree t's leaf
+// order (slice t of Xq, nrm, scl).  The positions and leaves of RB points
+// and up to 32 / RB trees are loaded by one lane each and broadcast.
+//
+// BF16 output: the centred row rounded to BF16 (d_pad elements, zero-padded).
+// E4M3 output (FP8): the centred row divided by its scale
+// s = max|x - c| / 448 (448 = largest finite E4M3 value) and rounded to E4M3
+// with saturation (d_pad bytes, zero-padded); the scale goes to `scl`.  In
+// both cases `nrm` receives the squared norm of the row the tensor cores see
+// (dequantised for FP8), so that ||y||^2 - 2 x.y ranks the same values.
+template <int NCH>
+struct StageCfg {
+  static constexpr int rb = NCH <= 2 ? 4 / NCH : 1;           // points per warp step
+  static constexpr int min_blocks = NCH == 1 ? 4 : (NCH == 2 ? 3 : 2);
+};
+
 template <typename T, int NCH, bool FP8>
-__global__ void __launch_bounds__(256) k_leaf_center(const T *__restrict__ X, int d, int d_pad,
-                                                     const int32_t *__restrict__ order,
-                                                     const int32_t *__restrict__ goff,
-                                                     const float *__restrict__ mu_in,
-                                                     void *__restrict__ Xq,
-                                                     float *__restrict__ nrm,
-                                                     float *__restrict__ scl) {
-  constexpr int W = NCH * 128;
-  __shared__ float mu[W];
-  const int j = blockIdx.x;
-  const int32_t lo = goff[j], hi = goff[j + 1];
-  const int m = hi - lo;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int i = threadIdx.x; i < W; i += 256) mu[i] = i < d ? __ldg(mu_in + (int64_t)j * d + i) : 0.0f;
-  __syncthreads();
-  constexpr int RB = NCH <= 2 ? 4 : 1;  // rows per warp step, loaded together
-  const int rb = (int)((int64_t)m * blockIdx.y / gridDim.y);
-  const int re = (int)((int64_t)m * (blockIdx.y + 1) / gridDim.y);
-  for (int r0w = rb + warp * RB; r0w < re; r0w += 8 * RB) {
+__global__ void __launch_bounds__(256, StageCfg<NCH>::min_blocks) k_leaf_stage(const T *__restrict__ X, int64_t n, int d,
+                                                    int d_pad, const int32_t *__restrict__ pos,
+                                                    const int32_t *__restrict__ lf,
+                                                    const float *__restrict__ mu, int nleaf,
+                                                    int tc, void *__restrict__ Xq,
+                                                    float *__restrict__ nrm,
+                                                    float *__restrict__ scl) {
+  constexpr int RB = StageCfg<NCH>::rb;  // points per warp step, loaded together
+  constexpr int TG = 32 / RB;            // trees per broadcast group
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r0 = gw * RB; r0 < n; r0 += nw * RB) {
     float v[RB][NCH][4];
 #pragma unroll
     for (int q = 0; q < RB; ++q) {
-      const int r = r0w + q;
-      const T *src = r < re ? X + (int64_t)__ldg(order + lo + r) * d : nullptr;
+      const int64_t r = r0 + q;
+      const T *src = r < n ? X + r * d : nullptr;
 #pragma unroll
       for (int h = 0; h < NCH; ++h) {
         const int c0 = h * 128 + 4 * lane;
         v[q][h][0] = v[q][h][1] = v[q][h][2] = v[q][h][3] = 0.0f;
-        if (src && c0 < d) load4<T>(src + c0, v[q][h]);
+        if (src && c0 < d) load4_cs<T>(src + c0, v[q][h]);
       }
     }
-#pragma unroll
-    for (int q = 0; q < RB; ++q) {
-      const int r = r0w + q;
-      const int64_t row = lo + (r < re ? r : 0);
-      float c[NCH][4];
-#pragma unroll
-      for (int h = 0; h < NCH; ++h)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int col = h * 128 + 4 * lane + e;
-          c[h][e] = col < d ? v[q][h][e] - mu[col] : 0.0f;
+    for (int tg = 0; tg < tc; tg += TG) {
+      int32_t my_pos = -1, my_lf = 0;
+      {
+        const int tt = tg + lane / RB;
+        const int64_t r = r0 + lane % RB;
+        if (lane < TG * RB && tt < tc && r < n) {
+          my_pos = __ldg(pos + (int64_t)tt * n + r);
+          my_lf = __ldg(lf + (int64_t)tt * n + r);
         }
-      float sq = 0.0f;
-      if constexpr (FP8) {
-        float amax = 0.0f;
+      }
+      const int tend = min(tg + TG, tc);
+      for (int t = tg; t < tend; ++t) {
+        // the RB points' leaf centres are all requested before the first use
+        int32_t rows[RB];
+        float m4[RB][NCH][4];
 #pragma unroll
-        for (int h = 0; h < NCH; ++h)
+        for (int q = 0; q < RB; ++q) {
+          const int src_lane = (t - tg) * RB + q;
+          rows[q] = __shfl_sync(kFull, my_pos, src_lane);
+          const int32_t leaf = __shfl_sync(kFull, my_lf, src_lane);  // 0 past the end
+          const float *mr = mu + ((int64_t)t * nleaf + leaf) * d;
 #pragma unroll
-          for (int e = 0; e < 4; ++e) amax = fmaxf(amax, fabsf(c[h][e]));
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(kFull, amax, o));
-        const float sc = amax > 0.0f ? amax / 448.0f : 1.0f;
-        const float inv = amax > 0.0f ? 448.0f / amax : 1.0f;
-        uint8_t *dst = static_cast<uint8_t *>(Xq) + row * d_pad;
-#pragma unroll
-        for (int h = 0; h < NCH; ++h) {
-          const int c0 = h * 128 + 4 * lane;
-          if (c0 < d_pad) {
-            const __nv_fp8x2_storage_t lo2 = __nv_cvt_float2_to_fp8x2(
-                make_float2(c[h][0] * inv, c[h][1] * inv), __NV_SATFINITE, __NV_E4M3);
-            const __nv_fp8x2_storage_t hi2 = __nv_cvt_float2_to_fp8x2(
-                make_float2(c[h][2] * inv, c[h][3] * inv), __NV_SATFINITE, __NV_E4M3);
-            const float2 a = __half22float2(__nv_cvt_fp8x2_to_halfraw2(lo2, __NV_E4M3));
-            const float2 b = __half22float2(__nv_cvt_fp8x2_to_halfraw2(hi2, __NV_E4M3));
-            sq = fmaf(a.x, a.x, sq);
-            sq = fmaf(a.y, a.y, sq);
-            sq = fmaf(b.x, b.x, sq);
-            sq = fmaf(b.y, b.y, sq);
-            if (r < re)
-              *reinterpret_cast<uint32_t *>(dst + c0) = (uint32_t)lo2 | ((uint32_t)hi2 << 16);
+          for (int h = 0; h < NCH; ++h) {
+            const int c0 = h * 128 + 4 * lane;
+            m4[q][h][0] = m4[q][h][1] = m4[q][h][2] = m4[q][h][3] = 0.0f;
+            if (c0 < d) load4<float>(mr + c0, m4[q][h]);
           }
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(kFull, sq, o);
-        if (lane == 0 && r < re) {
-          nrm[lo + r] = sq * sc * sc;
-          scl[lo + r] = sc;
-        }
-      } else {
-        __nv_bfloat16 *dst = static_cast<__nv_bfloat16 *>(Xq) + row * d_pad;
+        for (int q = 0; q < RB; ++q) {
+          const int32_t row = rows[q];
+          if (row < 0) continue;  // warp-uniform: a point past the end
+          float c[NCH][4];
 #pragma unroll
-        for (int h = 0; h < NCH; ++h) {
-          const int c0 = h * 128 + 4 * lane;
-          if (c0 < d_pad) {
-            __nv_bfloat16 b[4];
+          for (int h = 0; h < NCH; ++h) {
+            const int c0 = h * 128 + 4 * lane;
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              b[e] = __float2bfloat16_rn(c[h][e]);
-              const float vr = __bfloat162float(b[e]);
-              sq = fmaf(vr, vr, sq);
+            for (int e = 0; e < 4; ++e) c[h][e] = c0 + e < d ? v[q][h][e] - m4[q][h][e] : 0.0f;
+          }
+          const int64_t orow = (int64_t)t * n + row;
+          float sq = 0.0f;
+          if constexpr (FP8) {
+            float amax = 0.0f;
+#pragma unroll
+            for (int h = 0; h < NCH; ++h)
+#pragma unroll
+              for (int e = 0; e < 4; ++e) amax = fmaxf(amax, fabsf(c[h][e]));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(kFull, amax, o));
+            const float sc = amax > 0.0f ? amax / 448.0f : 1.0f;
+            const float inv = amax > 0.0f ? 448.0f / amax : 1.0f;
+            uint8_t *dst = static_cast<uint8_t *>(Xq) + orow * d_pad;
+#pragma unroll
+            for (int h = 0; h < NCH; ++h) {
+              const int c0 = h * 128 + 4 * lane;
+              if (c0 < d_pad) {
+                const __nv_fp8x2_storage_t lo2 = __nv_cvt_float2_to_fp8x2(
+                    make_float2(c[h][0] * inv, c[h][1] * inv), __NV_SATFINITE, __NV_E4M3);
+                const __nv_fp8x2_storage_t hi2 = __nv_cvt_float2_to_fp8x2(
+                    make_float2(c[h][2] * inv, c[h][3] * inv), __NV_SATFINITE, __NV_E4M3);
+                const float2 a = __half22float2(__nv_cvt_fp8x2_to_halfraw2(lo2, __NV_E4M3));
+                const float2 b = __half22float2(__nv_cvt_fp8x2_to_halfraw2(hi2, __NV_E4M3));
+                sq = fmaf(a.x, a.x, sq);
+                sq = fmaf(a.y, a.y, sq);
+                sq = fmaf(b.x, b.x, sq);
+                sq = fmaf(b.y, b.y, sq);
+                __stcs(reinterpret_cast<unsigned int *>(dst + c0),
+                       (unsigned int)lo2 | ((unsigned int)hi2 << 16));
+              }
             }
-            if (r < re) *reinterpret_cast<uint2 *>(dst + c0) = *reinterpret_cast<const uint2 *>(b);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(kFull, sq, o);
+            if (lane == 0) {
+              __stcs(nrm + orow, sq * sc * sc);
+              __stcs(scl + orow, sc);
+            }
+          } else {
+            __nv_bfloat16 *dst = static_cast<__nv_bfloat16 *>(Xq) + orow * d_pad;
+#pragma unroll
+            for (int h = 0; h < NCH; ++h) {
+              const int c0 = h * 128 + 4 * lane;
+              if (c0 < d_pad) {
+                __nv_bfloat16 b[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                  b[e] = __float2bfloat16_rn(c[h][e]);
+                  const float vr = __bfloat162float(b[e]);
+                  sq = fmaf(vr, vr, sq);
+                }
+                __stcs(reinterpret_cast<uint2 *>(dst + c0), *reinterpret_cast<const uint2 *>(b));
+              }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(kFull, sq, o);
+            if (lane == 0) __stcs(nrm + orow, sq);
           }
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(kFull, sq, o);
-        if (lane == 0 && r < re) nrm[lo + r] = sq;
       }
     }
   }
@@ -1032,27 +1103,49 @@ drpt_status make_tmap(CUtensorMap *map, const void *base, int64_t rows, int d_pa
 }
 
 template <typename T, int NCH>
-void center_t(const MixedTreeArgs &a, cudaStream_t s) {
-  // about 128 rows per block (at most 64 blocks per leaf), so that uneven
-  // leaf sizes do not leave a tail of long blocks
-  const int64_t mean = a.n / a.nleaf;
-  const int64_t split = std::max<int64_t>(1, std::min<int64_t>(64, mean / 128));
-  const dim3 grid((unsigned)a.nleaf, (unsigned)split);
-  k_leaf_mean<T, NCH><<<(unsigned)a.nleaf, 256, 0, s>>>((const T *)a.X, a.d, a.order, a.goff,
-                                                       a.mu);
+void stage_t(const LeafStageArgs &a, bool means, cudaStream_t s) {
+  const T *X = (const T *)a.X;
+  if (means) {
+    const dim3 g((unsigned)a.nleaf, (unsigned)a.T);
+    k_leaf_index<<<g, 256, 0, s>>>(a.order, a.goff, a.n, a.nleaf, a.pos, a.lf);
+    k_leaf_mean<T, NCH><<<g, 256, 0, s>>>(X, a.n, a.d, a.order, a.goff, a.nleaf, a.mu);
+    return;
+  }
+  constexpr int RB = StageCfg<NCH>::rb;
+  // one resident round of blocks, each warp looping over its points
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    auto kern = a.fp8 ? k_leaf_stage<T, NCH, true> : k_leaf_stage<T, NCH, false>;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+  }
+  int sms = 148;
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const unsigned grid =
+      (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(a.n, 8 * RB), (int64_t)sms * per_sm));
+  const int64_t toff = (int64_t)a.t0 * a.n;
+  const float *mu = a.mu + (int64_t)a.t0 * a.nleaf * a.d;
   if (a.fp8)
-    k_leaf_center<T, NCH, true><<<grid, 256, 0, s>>>((const T *)a.X, a.d, a.d_pad, a.order,
-                                                     a.goff, a.mu, a.Xb, a.nrm, a.scl);
+    k_leaf_stage<T, NCH, true><<<grid, 256, 0, s>>>(X, a.n, a.d, a.d_pad, a.pos + toff,
+                                                    a.lf + toff, mu, a.nleaf, a.tc, a.Xb, a.nrm,
+                                                    a.scl);
   else
-    k_leaf_center<T, NCH, false><<<grid, 256, 0, s>>>((const T *)a.X, a.d, a.d_pad, a.order,
-                                                      a.goff, a.mu, a.Xb, a.nrm, a.scl);
+    k_leaf_stage<T, NCH, false><<<grid, 256, 0, s>>>(X, a.n, a.d, a.d_pad, a.pos + toff,
+                                                     a.lf + toff, mu, a.nleaf, a.tc, a.Xb, a.nrm,
+                                                     a.scl);
 }
 
 template <typename T>
-void center_d(const MixedTreeArgs &a, cudaStream_t s) {
-  if (a.d_pad <= 256) center_t<T, 2>(a, s);
-  else if (a.d_pad <= 512) center_t<T, 4>(a, s);
-  else center_t<T, 8>(a, s);
+void stage_d(const LeafStageArgs &a, bool means, cudaStream_t s) {
+  if (a.d_pad <= 128) stage_t<T, 1>(a, means, s);
+  else if (a.d_pad <= 256) stage_t<T, 2>(a, means, s);
+  else if (a.d_pad <= 512) stage_t<T, 4>(a, means, s);
+  else stage_t<T, 8>(a, means, s);
 }
 
 template <int KP, bool STREAM, bool FP8>
@@ -1092,15 +1185,35 @@ drpt_status mma_kp(const MixedTreeArgs &a, const CUtensorMap &tmA, int kb, cudaS
 // K blocks (64 BF16 or 128 E4M3 values).
 int mixed_d_pad(int d, int fp8) { return fp8 ? (d + 127) / 128 * 128 : (d + 63) / 64 * 64; }
 
-drpt_status launch_leaf_center(const MixedTreeArgs &a, cudaStream_t s) {
+static drpt_status stage_check(const LeafStageArgs &a) {
   if (a.d % 4 != 0 || a.d > 1024 || a.d_pad != mixed_d_pad(a.d, a.fp8)) {
     set_error("mixed mode needs d %% 4 == 0 and d <= 1024 (got %d)", a.d);
     return DRPT_ERR_UNSUPPORTED;
   }
-  if (a.dtype == DRPT_DTYPE_U8) center_d<uint8_t>(a, s);
-  else center_d<float>(a, s);
+  return DRPT_OK;
+}
+
+drpt_status launch_leaf_means(const LeafStageArgs &a, cudaStream_t s) {
+  DRPT_TRY(stage_check(a));
+  if (a.dtype == DRPT_DTYPE_U8) stage_d<uint8_t>(a, true, s);
+  else stage_d<float>(a, true, s);
   DRPT_LAUNCH_CHECK();
   return DRPT_OK;
+}
+
+drpt_status launch_leaf_stage(const LeafStageArgs &a, cudaStream_t s) {
+  DRPT_TRY(stage_check(a));
+  if (a.dtype == DRPT_DTYPE_U8) stage_d<uint8_t>(a, false, s);
+  else stage_d<float>(a, false, s);
+  DRPT_LAUNCH_CHECK();
+  return DRPT_OK;
+}
+
+int mixed_stage_trees(int64_t n, int d_pad, int fp8, int T) {
+  // centred rows of as many trees as fit in 8 GiB
+  const int64_t per_tree = n * d_pad * (fp8 ? 1 : 2);
+  const int64_t fit = per_tree > 0 ? ((int64_t)8 << 30) / per_tree : T;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(T, fit));
 }
 
 drpt_status launch_leaf_mma(const MixedTreeArgs &a, cudaStream_t s) {

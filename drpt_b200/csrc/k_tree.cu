@@ -68,12 +68,15 @@ __device__ void node_bounds(float mu, float sigma, float *D) {
 
 // Slot of x (math_operations.cpp:292-308): slot j in 1..15 when
 // D[j-1] < x <= D[j]; slot 0 when no slot takes it.  D[0..13] never
-// decrease and (D[13], 0] cannot overlap them, so at most one j matches.
+// decrease (offsets from the mean in increasing order, rounded
+// monotonically) and D[14] = D[15] = 0, so for x <= D[13] the slot is the
+// number of D[0..12] below x (0 when x <= D[0], and for a NaN x); above
+// D[13] only slot 14 can take x, when x <= 0.
 __device__ __forceinline__ int bin_of(const float *D, float x) {
+  if (x > D[13]) return x <= 0.0f ? 14 : 0;
   int slot = 0;
 #pragma unroll
-  for (int j = 1; j < kBins; ++j)
-    if (D[j - 1] < x && D[j] >= x) slot = j;
+  for (int j = 0; j < 13; ++j) slot += D[j] < x ? 1 : 0;
   return slot;
 }
 
@@ -312,6 +315,9 @@ __global__ void k_bounds_fast(TreeLevelArgs a) {
 }
 
 // ------------------------------------------------------------------ histogram
+// Per thread, the 16 counts are 16-bit fields of four 64-bit registers
+// (at most kPer values per thread and kUnit per warp sum, both below 2^16),
+// added over the warp with shuffles; no atomics.
 __global__ void __launch_bounds__(kThreads) k_hist(TreeLevelArgs a) {
   __shared__ unsigned hist[kWarps][kBins];
   __shared__ float Ds[kBins];
@@ -324,13 +330,25 @@ __global__ void __launch_bounds__(kThreads) k_hist(TreeLevelArgs a) {
     const int len = (int)min64(kUnit, r.hi - lo);
     const float *v = tree_vals(a, t) + lo;
     if (threadIdx.x < kBins) Ds[threadIdx.x] = a.node_D[(int64_t)g * kBins + threadIdx.x];
-    for (int i = threadIdx.x; i < kWarps * kBins; i += kThreads) (&hist[0][0])[i] = 0u;
     __syncthreads();
     float D[kBins];
 #pragma unroll
     for (int j = 0; j < kBins; ++j) D[j] = Ds[j];
-    const int w = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < len; i += kThreads) atomicAdd(&hist[w][bin_of(D, __ldg(v + i))], 1u);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint64_t c4[4] = {0ull, 0ull, 0ull, 0ull};
+    for (int i = threadIdx.x; i < len; i += kThreads) {
+      const int b = bin_of(D, __ldg(v + i));
+      const uint64_t inc = 1ull << (16 * (b & 3));
+#pragma unroll
+      for (int q = 0; q < 4; ++q) c4[q] += (b >> 2) == q ? inc : 0ull;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) c4[q] += __shfl_xor_sync(kFull, c4[q], o);
+    const int q = lane >> 2;
+    const uint64_t mine = q == 0 ? c4[0] : q == 1 ? c4[1] : q == 2 ? c4[2] : c4[3];
+    if (lane < kBins) hist[w][lane] = (unsigned)((mine >> (16 * (lane & 3))) & 0xffffu);
     __syncthreads();
     if (threadIdx.x < kBins) {
       unsigned tot = 0;

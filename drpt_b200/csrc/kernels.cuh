@@ -106,18 +106,35 @@ struct MixedTreeArgs {
   void *Xb;                  // n x d_pad centred rows in leaf order (BF16 or E4M3)
   float *nrm;                // n, squared norms of the rows the tensor cores see
   float *scl;                // n, per-row E4M3 scales (FP8 only)
-  float *mu;                 // nleaf x d, leaf centres
   int32_t *tile_leaf, *tile_r0, *n_tiles;  // n / 128 + nleaf
   int32_t *cand_idx;         // n x kp running list (point ids), updated tree by tree
   float *cand_dist;          // n x kp approximate squared distances, ascending
   int *err;                  // set when a bounded wait gave up
 };
 int mixed_d_pad(int d, int fp8);
+// The mixed form's staging of centred rows for the trees t0 .. t0 + tc - 1
+// (launch_leaf_means covers every tree; launch_leaf_stage one chunk).
+struct LeafStageArgs {
+  const void *X;
+  int dtype;
+  int64_t n;
+  int d, d_pad, fp8;
+  const int32_t *order, *goff;  // every tree: T x n leaf orders, T x (nleaf + 1) starts
+  int nleaf, T;
+  int32_t *pos, *lf;            // T x n: each point's row in the tree's leaf order, its leaf
+  float *mu;                    // T x nleaf x d leaf centres
+  int t0, tc;                   // the chunk
+  void *Xb;                     // tc x n x d_pad centred rows, slice t in tree t0 + t's order
+  float *nrm, *scl;             // tc x n
+};
+drpt_status launch_leaf_means(const LeafStageArgs &a, cudaStream_t s);
+drpt_status launch_leaf_stage(const LeafStageArgs &a, cudaStream_t s);
+// trees per staging chunk: as many as 8 GiB of centred rows hold, at least 1
+int mixed_stage_trees(int64_t n, int d_pad, int fp8, int T);
 // Batches: ids of point p's neighbours made relative to its dataset's first
 // row (set_off: nsets + 1 row offsets, device).
 drpt_status launch_localize(int32_t *idx, int64_t n, int k, const int64_t *set_off, int nsets,
                             cudaStream_t s);
-drpt_status launch_leaf_center(const MixedTreeArgs &a, cudaStream_t s);
 drpt_status launch_leaf_mma(const MixedTreeArgs &a, cudaStream_t s);
 drpt_status launch_rerank(const void *X, int dtype, int d, const int32_t *visit, int64_t n,
                           const int32_t *cand, int K2, int k, int32_t *out_idx, float *out_dist,
