@@ -28,7 +28,7 @@ EXPORTS = [
     "drpt_host_projection", "drpt_project", "drpt_global_trees", "drpt_local_leaves",
     "drpt_leaf_knn", "drpt_merge_candidates", "drpt_global_trees_noalloc",
     "drpt_build_graph_batched", "drpt_learn_gradient", "drpt_index_build", "drpt_index_query",
-    "drpt_index_destroy",
+    "drpt_index_destroy", "drpt_locality_slots",
 ]
 
 
@@ -51,7 +51,7 @@ class BuildDesc(ctypes.Structure):
         ("data_on_device", ctypes.c_int32), ("out_on_device", ctypes.c_int32),
         ("stream", ctypes.c_void_p), ("leaf_size", ctypes.c_int32), ("precision", ctypes.c_int32),
         ("learned_trees", ctypes.c_int32), ("learn_sample", ctypes.c_int32),
-        ("learn_iters", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("learn_iters", ctypes.c_int32), ("locality", ctypes.c_int32),
     ]
 
 
@@ -113,6 +113,7 @@ def load(path: str = LIB_PATH):
         L.drpt_project.argtypes = [vp, vp, i64, i32, i32, vp, i32, vp, i32, vp, vp]
         L.drpt_global_trees.argtypes = [vp, vp, i64, i32, i32, i32, vp, vp, vp, vp]
         L.drpt_local_leaves.argtypes = [vp, vp, vp, i64, i32, i32, i32, vp, vp, vp]
+        L.drpt_locality_slots.argtypes = [vp, vp, i64, i32, i32, vp, vp, vp]
         L.drpt_leaf_knn.argtypes = [vp, vp, i32, i64, i32, i32, vp, vp, i32, i32, vp, vp, vp]
         L.drpt_merge_candidates.argtypes = [vp, vp, vp, i64, i32, i32, vp, vp, vp]
         L.drpt_global_trees_noalloc.argtypes = [vp, i64, i32, i32, i32, vp, vp, vp, vp]

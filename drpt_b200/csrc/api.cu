@@ -1559,6 +1559,20 @@ static drpt_status build_graph_impl(drpt_ctx *c, const drpt_build_desc *desc, co
   DRPT_TRY(global_trees(c, P, n, T, g.gd, exact, nullptr, &order, &goff, s));
   DRPT_CUDA(cudaEventRecord(ev[2], s));
 
+  if (desc->locality) {
+    // locality relabelling on the host: every tree's global leaves in slot order
+    const size_t no = (size_t)T * n, nf = (size_t)T * (g.nleaf + 1);
+    std::vector<int32_t> ho(no), hf(nf), so(no), sf(nf), slots((size_t)g.nleaf * T);
+    DRPT_CUDA(cudaMemcpyAsync(ho.data(), order, no * 4, cudaMemcpyDeviceToHost, s));
+    DRPT_CUDA(cudaMemcpyAsync(hf.data(), goff, nf * 4, cudaMemcpyDeviceToHost, s));
+    DRPT_CUDA(cudaStreamSynchronize(s));
+    DRPT_TRY(drpt_locality_slots(ho.data(), hf.data(), n, T, g.nleaf, slots.data(), so.data(),
+                                 sf.data()));
+    DRPT_CUDA(cudaMemcpyAsync(order, so.data(), no * 4, cudaMemcpyHostToDevice, s));
+    DRPT_CUDA(cudaMemcpyAsync(goff, sf.data(), nf * 4, cudaMemcpyHostToDevice, s));
+    DRPT_CUDA(cudaStreamSynchronize(s));
+  }
+
   // K5: local split (one host round trip for the leaf sizes).
   int32_t *forder, *foff;
   DRPT_TRY(ws_get(c, "final_order", (size_t)T * n, &forder));
@@ -1756,6 +1770,52 @@ drpt_status drpt_global_trees(drpt_ctx *c, const float *P, int64_t n, int32_t T,
   DRPT_CUDA(cudaMemcpyAsync(order, o, (size_t)T * n * 4, cudaMemcpyDeviceToDevice, s));
   DRPT_CUDA(cudaMemcpyAsync(offsets, f, (size_t)T * ((1 << (gd - 1)) + 1) * 4,
                             cudaMemcpyDeviceToDevice, s));
+  return DRPT_OK;
+}
+
+drpt_status drpt_locality_slots(const int32_t *order, const int32_t *offsets, int64_t n, int32_t T,
+                                int32_t nleaf, int32_t *slot_leaf, int32_t *order_out,
+                                int32_t *offsets_out) {
+  if (!order || !offsets || !slot_leaf || n < 1 || n > INT32_MAX || T <= 0 || nleaf <= 0 ||
+      (nleaf & (nleaf - 1)) != 0 || (!order_out) != (!offsets_out)) {
+    set_error("locality: invalid arguments");
+    return DRPT_ERR_INVALID_ARG;
+  }
+  for (int t = 0; t < T; ++t) {
+    const int32_t *o = offsets + (size_t)t * (nleaf + 1);
+    if (o[0] != 0 || o[nleaf] != n) {
+      set_error("locality: tree %d's leaf offsets do not cover the %lld points", t, (long long)n);
+      return DRPT_ERR_INVALID_ARG;
+    }
+    for (int j = 0; j < nleaf; ++j)
+      if (o[j + 1] < o[j]) {
+        set_error("locality: tree %d's leaf offsets decrease", t);
+        return DRPT_ERR_INVALID_ARG;
+      }
+  }
+  for (size_t i = 0; i < (size_t)T * n; ++i)
+    if (order[i] < 0 || order[i] >= n) {
+      set_error("locality: point id %d out of range", order[i]);
+      return DRPT_ERR_INVALID_ARG;
+    }
+  if (!host_locality_slots(T, nleaf, n, order, offsets, slot_leaf)) {
+    set_error("locality: a slot found no free leaf (the reference reads index -1 there)");
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  if (order_out) {
+    for (int t = 0; t < T; ++t) {
+      const int32_t *o = offsets + (size_t)t * (nleaf + 1);
+      int32_t *oo = offsets_out + (size_t)t * (nleaf + 1);
+      int32_t w = 0;
+      oo[0] = 0;
+      for (int k = 0; k < nleaf; ++k) {
+        const int leaf = slot_leaf[(size_t)k * T + t];
+        for (int32_t i = o[leaf]; i < o[leaf + 1]; ++i)
+          order_out[(size_t)t * n + w++] = order[(size_t)t * n + i];
+        oo[k + 1] = w;
+      }
+    }
+  }
   return DRPT_OK;
 }
 

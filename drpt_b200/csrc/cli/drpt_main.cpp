@@ -12,9 +12,9 @@
 // Flags added here: -seed (projection seed; default drawn from
 // std::random_device as the reference draws it, mdrpt.cpp:402-416, and
 // printed), -mode exact|fast|mixed|fp32_leaf (default exact), -leaf-size,
-// -tree-depth, -device.  -locality is accepted and has no effect: at one
-// rank the reference's locality pass relabels leaves and the graph is the
-// same.
+// -tree-depth, -device.  -locality 1 runs the reference's locality
+// relabelling in the exact and fast modes (off unless given: at one rank it
+// only renumbers global leaves and the graph is the same).
 //
 // Input formats (-data-file-format), plain or gzip-compressed:
 //   0  IDX3 ubyte (file_reader.cpp:33-83): big-endian header magic 0x803,
@@ -59,6 +59,7 @@ struct Options {
   int mode = DRPT_MODE_EXACT;
   int precision = DRPT_PRECISION_BF16;
   int learned_trees = 0;
+  int locality = 0;
   bool write_distances = false;
 };
 
@@ -87,7 +88,7 @@ Options parse(int argc, char **argv) {
     else if (!std::strcmp(f, "-tree-depth-ratio")) o.tree_depth_ratio = std::strtof(v, nullptr);
     else if (!std::strcmp(f, "-density")) o.density = std::strtod(v, nullptr);
     else if (!std::strcmp(f, "-nn")) o.nn = std::atoi(v);
-    else if (!std::strcmp(f, "-locality")) (void)std::atoi(v);
+    else if (!std::strcmp(f, "-locality")) o.locality = std::atoi(v) == 1 ? 1 : 0;
     else if (!std::strcmp(f, "-local-tree-offset")) o.local_tree_offset = std::atoi(v);
     else if (!std::strcmp(f, "-data-file-format")) o.file_format = std::atoi(v);
     else if (!std::strcmp(f, "-bytes-for-data-type")) o.bytes_for_data_type = std::atoi(v);
@@ -250,6 +251,7 @@ int main(int argc, char **argv) {
   desc.leaf_size = o.leaf_size;
   desc.precision = o.precision;
   desc.learned_trees = o.learned_trees;
+  desc.locality = o.locality;
   std::vector<int32_t> idx((size_t)o.n * o.nn);
   std::vector<float> dist(o.write_distances ? (size_t)o.n * o.nn : 0);
   drpt_stats st;

@@ -1,7 +1,7 @@
 // Host-side parts of the path that the reference computes with libstdc++:
-// the seeded projection matrix and the positional local split.  Both call
-// the same libstdc++ facilities the reference calls, so they reproduce its
-// results bit for bit on the same standard library.
+// the seeded projection matrix, the positional local split and the locality
+// relabelling.  They call the same libstdc++ facilities the reference calls,
+// so they reproduce its results bit for bit on the same standard library.
 #pragma once
 
 #include <stdint.h>
@@ -23,5 +23,13 @@ bool host_local_matrix_is_zero(uint32_t seed, int d, int L);
 // first has 2^ld + 1 entries (leaf starts).
 void host_local_permutation(int64_t n, int ld, std::vector<int32_t> &perm,
                             std::vector<int32_t> &first);
+
+// The locality relabelling of the global leaves at one rank and one thread
+// (drpt_global.cpp:64-151, 572-732).  order (T x n) and goff (T x (nleaf + 1))
+// are every tree's global leaves; slot_leaf[k * T + t] receives the leaf of
+// tree t placed at slot k.  Returns false when a slot finds no free leaf
+// (the reference then indexes its tables with -1).
+bool host_locality_slots(int T, int nleaf, int64_t n, const int32_t *order, const int32_t *goff,
+                         int32_t *slot_leaf);
 
 }  // namespace drpt

@@ -62,7 +62,8 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
                 tree_depth_ratio: float = 0.6, local_tree_offset: int = 2, tree_depth: int = 0,
                 density: float = 0.0, local_seeds=None, device: int = 0, stream=None,
                 out=None, leaf_size: int = 0, precision: str = "bf16", learned_trees: int = 0,
-                learn_sample: int = 0, learn_iters: int = 0, _index_out=None):
+                learn_sample: int = 0, learn_iters: int = 0, locality: bool = False,
+                _index_out=None):
     """k-NN graph of `data` (n x d, uint8 or float32; a NumPy array in host
     memory or a CUDA tensor).  Returns (idx, dist, stats): idx int32 and dist
     float32 of shape (n, nn), each point's nn nearest distinct neighbours other
@@ -72,7 +73,9 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
     the operand type of the mixed form's tensor-core leaf tiles; the last
     `learned_trees` of the `ntrees` trees split on learned MLP values trained
     on a sample of `learn_sample` points (0 = 8,192) with `learn_iters` Adam
-    steps per level (0 = 10)."""
+    steps per level (0 = 10).  `locality` (exact and fast modes) runs the
+    reference's locality relabelling of the global leaves; at one rank the
+    graph is the same either way."""
     on_dev = _is_cuda_tensor(data)
     if not on_dev:
         data = np.ascontiguousarray(data)
@@ -95,6 +98,7 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
     desc.precision = {"bf16": _lib.PRECISION_BF16, "fp8": _lib.PRECISION_FP8_E4M3}[precision]
     desc.learned_trees, desc.learn_sample = learned_trees, learn_sample
     desc.learn_iters = learn_iters
+    desc.locality = 1 if locality else 0
     desc.data_on_device = 1 if on_dev else 0
     desc.out_on_device = desc.data_on_device
     if on_dev:
@@ -279,9 +283,10 @@ class MDRPT:
 
     def grow_trees(self, original_data, density: float, use_locality_optimization: bool, nn: int):
         """Projection, global trees and positional local split
-        (mdrpt.cpp:46-121).  At one rank the locality optimisation only
-        relabels leaves and leaves the graph unchanged; it is accepted and
-        has no effect here."""
+        (mdrpt.cpp:46-121).  With `use_locality_optimization` the global
+        leaves are put in the reference's locality slot order
+        (drpt_global.cpp:572-732) before the local split; at one rank that
+        only renumbers leaves, the graph is the same."""
         torch = _torch()
         dev = torch.device("cuda", self.device)
         X = original_data if _is_cuda_tensor(original_data) else \
@@ -313,6 +318,16 @@ class MDRPT:
         check(self._L.drpt_global_trees(self._ctx.handle, P.data_ptr(), n, T, gd,
                                         1 if self.exact else 0, order.data_ptr(), offs.data_ptr(),
                                         med.data_ptr(), s))
+        if use_locality_optimization:
+            ho = np.ascontiguousarray(order.cpu().numpy())
+            hf = np.ascontiguousarray(offs.cpu().numpy())
+            slots = np.empty((nleaf, T), np.int32)
+            so, sf = np.empty_like(ho), np.empty_like(hf)
+            check(self._L.drpt_locality_slots(ho.ctypes.data, hf.ctypes.data, n, T, nleaf,
+                                              slots.ctypes.data, so.ctypes.data, sf.ctypes.data))
+            self.locality_slots = slots
+            order = torch.from_numpy(so).to(dev)
+            offs = torch.from_numpy(sf).to(dev)
         self.P, self.global_order, self.global_offsets, self.medians = P, order, offs, med
         sizes = (offs[:, 1:] - offs[:, :-1]).cpu().numpy()
         nonempty = sizes[sizes > 0]

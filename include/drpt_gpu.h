@@ -112,7 +112,10 @@ typedef struct {
   int32_t learn_sample;       /* sample points the split MLPs train on
                                  (0 = 8,192) */
   int32_t learn_iters;        /* Adam steps per level (0 = 10) */
-  int32_t reserved;
+  int32_t locality;           /* exact and fast modes: 1 runs the locality
+                                 relabelling (-locality 1) between the global
+                                 and the local trees; at one rank it only
+                                 renumbers global leaves, the graph is the same */
 } drpt_build_desc;
 
 typedef struct {
@@ -244,6 +247,19 @@ drpt_status drpt_project(drpt_ctx *ctx, const void *X, int64_t n, int32_t d, int
 drpt_status drpt_global_trees(drpt_ctx *ctx, const float *P, int64_t n, int32_t T, int32_t gd,
                               int32_t exact, int32_t *order, int32_t *offsets, float *medians,
                               void *stream);
+
+/* Locality relabelling of the global leaves, one rank and one thread
+ * (replaces DRPTGlobal::calculate_tree_leaf_correlation, drpt_global.cpp:572-732,
+ * with sortByFreq and select_next_candidate, :64-151).  HOST memory: order and
+ * offsets as drpt_global_trees produces them (nleaf = 2^(gd-1));
+ * slot_leaf (nleaf x T) receives the leaf of tree t placed at slot k
+ * (final_tree_leaf_mapping).  When order_out and offsets_out are not NULL they
+ * receive every tree's leaves in slot order (trees_leaf_first_indices_rearrange).
+ * No device work.  DRPT_ERR_UNSUPPORTED when a slot finds no free leaf (the
+ * reference then reads its tables at index -1). */
+drpt_status drpt_locality_slots(const int32_t *order, const int32_t *offsets, int64_t n, int32_t T,
+                                int32_t nleaf, int32_t *slot_leaf, int32_t *order_out,
+                                int32_t *offsets_out);
 
 /* Positional local split of every global leaf (offsets as produced above) to
  * depth ld.  final_order (T x n), final_offsets (T x (2^(gd-1+ld)+1)). */

@@ -7,7 +7,8 @@ stand-in, the ordered cblas and seed injection).
 Each case_*.npz holds the seeded input, the run parameters and what the
 reference produced: the projection matrix B, P = X.B, every tree's final
 leaves (point ids in leaf order; P is omitted for the largest case plus leaf offsets, leaf ids in heap order with
--locality 0) and the first nn+4 entries of every point's merged neighbour
+-locality 0), the final leaves of the same run with -locality 1 (leaf ids in
+the locality pass's slot order) and the first nn+4 entries of every point's merged neighbour
 list exactly as gather_nns returned it (self and any duplicate entries
 included).  median_cases.npz holds per-node means, variances and medians from
 MathOp::distributed_mean/_variance/_median on hand-picked value sets,
@@ -117,6 +118,7 @@ def run_case(name: str, spec: dict, tmp: str) -> None:
         final_order=r["final_order"],
         final_offsets=r["final_offsets"], list_idx=lidx, list_dist=ldist, list_len=llen,
         locality_same_partition=same_partition, locality_same_lists=same_lists,
+        locality_final_order=r1["final_order"], locality_final_offsets=r1["final_offsets"],
         ref_stdout=out.strip().splitlines()[-1])
     print(f"{name}: n={n} d={d} gd={r['gd']} ld={r['ld']} n_final={r['n_final']} "
           f"locality partition/lists unchanged: {same_partition}/{same_lists} "

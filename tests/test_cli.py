@@ -112,6 +112,14 @@ def test_cli_graph_matches_reference(cli, tmp_path, case, fmt):
     res = knn_compare.compare(ri[:, :nn - 1], rd[:, :nn - 1], got, dist[:, :nn - 1], rd)
     assert res["fail"] == 0, res
     assert os.path.getsize(out + "stats.txt") > 0
+    # -locality 1 renumbers the global leaves only: the same edge list
+    out1 = str(tmp_path / "loc") + "/"
+    os.makedirs(out1)
+    r = _run(cli, "-input", path, "-output", out1, "-data-set-size", n, "-dimension", d,
+             "-ntrees", T, "-nn", nn, "-seed", seed, "-locality", 1, *extra)
+    assert r.returncode == 0, r.stdout + r.stderr
+    with open(out1 + "results.txt") as f:
+        assert f.read() == text
 
 
 def test_header_checks(cli, tmp_path):

@@ -30,13 +30,13 @@ def torch():
     return _t
 
 
-def _mdrpt(g, exact=True):
+def _mdrpt(g, exact=True, locality=False):
     X = g["X"]
     n, d = X.shape
     T, nn = int(g["ntrees"]), int(g["nn"])
     td, _ = global_depth(n)
     m = MDRPT(T, td, 0.6, 2, n, n, d, seed=int(g["seeds"][0]), exact=exact)
-    m.grow_trees(X, 0.0, False, nn)
+    m.grow_trees(X, 0.0, locality, nn)
     return m
 
 
@@ -72,6 +72,24 @@ def test_final_leaves_match_reference(torch, case):
     assert m.ld == int(g["ld"]) and m.n_final == int(g["n_final"])
     assert np.array_equal(m.final_offsets.cpu().numpy(), g["final_offsets"])
     assert np.array_equal(m.final_order.cpu().numpy(), g["final_order"])
+
+
+@pytest.mark.parametrize("case", OK_CASES, ids=_id)
+def test_locality_final_leaves_match_reference(torch, case):
+    """With the locality relabelling the final leaves come in the
+    reference's -locality 1 order: leaf ids, not only the partition."""
+    g = np.load(case)
+    m = _mdrpt(g, locality=True)
+    assert np.array_equal(m.final_offsets.cpu().numpy(), g["locality_final_offsets"])
+    assert np.array_equal(m.final_order.cpu().numpy(), g["locality_final_order"])
+    idx, dist = m.gather_nns(int(g["nn"]))
+    m0 = _mdrpt(g)
+    idx0, dist0 = m0.gather_nns(int(g["nn"]))
+    assert np.array_equal(idx.cpu().numpy(), idx0.cpu().numpy())
+    X = g["X"]
+    i1, d1, _ = build_graph(X, int(g["ntrees"]), int(g["nn"]), int(g["seeds"][0]), locality=True)
+    i2, d2, _ = build_graph(X, int(g["ntrees"]), int(g["nn"]), int(g["seeds"][0]))
+    assert np.array_equal(i1, i2) and np.array_equal(d1, d2)
 
 
 @pytest.mark.parametrize("case", OK_CASES, ids=_id)
