@@ -197,7 +197,8 @@ struct StageCfg {
   static constexpr int min_blocks = NCH == 1 ? 4 : (NCH == 2 ? 3 : 2);
 };
 
-template <typename T, int NCH, bool FP8>
+// FULL: d == d_pad == 128 * NCH, so no dimension needs a bounds check.
+template <typename T, int NCH, bool FP8, bool FULL>
 __global__ void __launch_bounds__(256, StageCfg<NCH>::min_blocks) k_leaf_stage(const T *__restrict__ X, int64_t n, int d,
                                                     int d_pad, const int32_t *__restrict__ pos,
                                                     const int32_t *__restrict__ lf,
@@ -220,7 +221,7 @@ __global__ void __launch_bounds__(256, StageCfg<NCH>::min_blocks) k_leaf_stage(c
       for (int h = 0; h < NCH; ++h) {
         const int c0 = h * 128 + 4 * lane;
         v[q][h][0] = v[q][h][1] = v[q][h][2] = v[q][h][3] = 0.0f;
-        if (src && c0 < d) load4_cs<T>(src + c0, v[q][h]);
+        if (src && (FULL || c0 < d)) load4_cs<T>(src + c0, v[q][h]);
       }
     }
     for (int tg = 0; tg < tc; tg += TG) {
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(256, StageCfg<NCH>::min_blocks) k_leaf_stage(c
           for (int h = 0; h < NCH; ++h) {
             const int c0 = h * 128 + 4 * lane;
             m4[q][h][0] = m4[q][h][1] = m4[q][h][2] = m4[q][h][3] = 0.0f;
-            if (c0 < d) load4<float>(mr + c0, m4[q][h]);
+            if (FULL || c0 < d) load4<float>(mr + c0, m4[q][h]);
           }
         }
 #pragma unroll
@@ -260,7 +261,8 @@ __global__ void __launch_bounds__(256, StageCfg<NCH>::min_blocks) k_leaf_stage(c
           for (int h = 0; h < NCH; ++h) {
             const int c0 = h * 128 + 4 * lane;
 #pragma unroll
-            for (int e = 0; e < 4; ++e) c[h][e] = c0 + e < d ? v[q][h][e] - m4[q][h][e] : 0.0f;
+            for (int e = 0; e < 4; ++e)
+              c[h][e] = (FULL || c0 + e < d) ? v[q][h][e] - m4[q][h][e] : 0.0f;
           }
           const int64_t orow = (int64_t)t * n + row;
           float sq = 0.0f;
@@ -278,7 +280,7 @@ __global__ void __launch_bounds__(256, StageCfg<NCH>::min_blocks) k_leaf_stage(c
 #pragma unroll
             for (int h = 0; h < NCH; ++h) {
               const int c0 = h * 128 + 4 * lane;
-              if (c0 < d_pad) {
+              if (FULL || c0 < d_pad) {
                 const __nv_fp8x2_storage_t lo2 = __nv_cvt_float2_to_fp8x2(
                     make_float2(c[h][0] * inv, c[h][1] * inv), __NV_SATFINITE, __NV_E4M3);
                 const __nv_fp8x2_storage_t hi2 = __nv_cvt_float2_to_fp8x2(
@@ -304,7 +306,7 @@ __global__ void __launch_bounds__(256, StageCfg<NCH>::min_blocks) k_leaf_stage(c
 #pragma unroll
             for (int h = 0; h < NCH; ++h) {
               const int c0 = h * 128 + 4 * lane;
-              if (c0 < d_pad) {
+              if (FULL || c0 < d_pad) {
                 __nv_bfloat16 b[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
@@ -1113,9 +1115,11 @@ void stage_t(const LeafStageArgs &a, bool means, cudaStream_t s) {
   }
   constexpr int RB = StageCfg<NCH>::rb;
   // one resident round of blocks, each warp looping over its points
-  static int per_sm = 0;
+  const bool full = a.d == NCH * 128 && a.d_pad == NCH * 128;
+  auto kern = a.fp8 ? (full ? k_leaf_stage<T, NCH, true, true> : k_leaf_stage<T, NCH, true, false>)
+                    : (full ? k_leaf_stage<T, NCH, false, true> : k_leaf_stage<T, NCH, false, false>);
+  static int per_sm = 0;  // the four forms use the same registers within a few
   if (per_sm == 0) {
-    auto kern = a.fp8 ? k_leaf_stage<T, NCH, true> : k_leaf_stage<T, NCH, false>;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0) != cudaSuccess ||
         per_sm < 1)
       per_sm = 1;
@@ -1130,14 +1134,8 @@ void stage_t(const LeafStageArgs &a, bool means, cudaStream_t s) {
       (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(a.n, 8 * RB), (int64_t)sms * per_sm));
   const int64_t toff = (int64_t)a.t0 * a.n;
   const float *mu = a.mu + (int64_t)a.t0 * a.nleaf * a.d;
-  if (a.fp8)
-    k_leaf_stage<T, NCH, true><<<grid, 256, 0, s>>>(X, a.n, a.d, a.d_pad, a.pos + toff,
-                                                    a.lf + toff, mu, a.nleaf, a.tc, a.Xb, a.nrm,
-                                                    a.scl);
-  else
-    k_leaf_stage<T, NCH, false><<<grid, 256, 0, s>>>(X, a.n, a.d, a.d_pad, a.pos + toff,
-                                                     a.lf + toff, mu, a.nleaf, a.tc, a.Xb, a.nrm,
-                                                     a.scl);
+  kern<<<grid, 256, 0, s>>>(X, a.n, a.d, a.d_pad, a.pos + toff, a.lf + toff, mu, a.nleaf, a.tc,
+                            a.Xb, a.nrm, a.scl);
 }
 
 template <typename T>

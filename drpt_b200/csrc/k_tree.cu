@@ -256,11 +256,21 @@ __global__ void __launch_bounds__(kThreads) k_stats_partial(TreeLevelArgs a) {
     const int64_t lo = a.unit_lo[u];
     const int len = (int)min64(kUnit, r.hi - lo);
     const float *v = tree_vals(a, t) + lo;
+    // all kPer loads of a thread in flight before the sums (same order of adds)
+    float xs[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      const int i = threadIdx.x + j * kThreads;
+      xs[j] = i < len ? __ldg(v + i) : 0.0f;
+    }
     double s1 = 0.0, s2 = 0.0;
-    for (int i = threadIdx.x; i < len; i += kThreads) {
-      const double x = (double)__ldg(v + i);
-      s1 += x;
-      s2 += x * x;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      if (threadIdx.x + j * kThreads < len) {
+        const double x = (double)xs[j];
+        s1 += x;
+        s2 += x * x;
+      }
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
@@ -336,11 +346,20 @@ __global__ void __launch_bounds__(kThreads) k_hist(TreeLevelArgs a) {
     for (int j = 0; j < kBins; ++j) D[j] = Ds[j];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint64_t c4[4] = {0ull, 0ull, 0ull, 0ull};
-    for (int i = threadIdx.x; i < len; i += kThreads) {
-      const int b = bin_of(D, __ldg(v + i));
-      const uint64_t inc = 1ull << (16 * (b & 3));
+    float xs[kPer];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) c4[q] += (b >> 2) == q ? inc : 0ull;
+    for (int j = 0; j < kPer; ++j) {
+      const int i = threadIdx.x + j * kThreads;
+      xs[j] = i < len ? __ldg(v + i) : 0.0f;
+    }
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      if (threadIdx.x + j * kThreads < len) {
+        const int b = bin_of(D, xs[j]);
+        const uint64_t inc = 1ull << (16 * (b & 3));
+#pragma unroll
+        for (int q = 0; q < 4; ++q) c4[q] += (b >> 2) == q ? inc : 0ull;
+      }
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q)
@@ -407,8 +426,16 @@ __global__ void __launch_bounds__(kThreads) k_count(TreeLevelArgs a) {
     const int len = (int)min64(kUnit, r.hi - lo);
     const float *v = tree_vals(a, t) + lo;
     const float med = a.node_med[g];
+    float xs[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      const int i = threadIdx.x + j * kThreads;
+      xs[j] = i < len ? __ldg(v + i) : 0.0f;
+    }
     int c = 0;
-    for (int i = threadIdx.x; i < len; i += kThreads) c += (__ldg(v + i) <= med) ? 1 : 0;  // :308
+#pragma unroll
+    for (int j = 0; j < kPer; ++j)  // value <= median goes left (drpt_global.cpp:308)
+      c += (threadIdx.x + j * kThreads < len && xs[j] <= med) ? 1 : 0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = c;
