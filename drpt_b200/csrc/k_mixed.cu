@@ -48,27 +48,33 @@ using namespace sm100;
 constexpr int kTM = 128;            // rows per tile (M)
 constexpr int kTN = 64;             // columns per tile (N) of the streamed form
 // Per list width KP and A layout: columns per tile (N), accumulator buffers
-// (together 128 TMEM columns), B-tile stages, per-row pending-key slots and
-// the CTAs per SM the kernel is built for.  The epilogue bounds the kernel,
-// so the configurations maximise epilogue warps per SM: with 16 keys per row
-// and a resident A, 3 CTAs share an SM (d <= 128: 66 KB of shared memory
-// each) on one 64-column B stage and 32 slots.  (Three 32-column stages and
-// four accumulators in the same space measured slower: twice the per-tile
-// epilogue overhead.)  With 32 keys, 2 CTAs, two stages and 64 slots.
+// (together 128 TMEM columns), B-tile stages, per-row pending-key slots,
+// epilogue groups of four warps and the CTAs per SM the kernel is built for.
+// The epilogue bounds the kernel: with 16 keys per row and a resident A,
+// one group, 3 CTAs per SM (d <= 128: 68 KB of shared memory each) on one
+// 64-column B stage and 32 slots.  Measured slower on the 1M x 128 bench
+// build (leaf kernel, 6 trees): two groups taking the column tiles in turn
+// at 2 CTAs per SM (5.96 ms against 4.96: their split lists need more
+// flushes), three 32-column stages with four accumulators (5.35 ms: twice
+// the per-tile epilogue overhead), one group at 2 CTAs per SM with two or
+// three stages (5.48 ms).  With 32 keys or a streamed A: one group, 2 CTAs,
+// two stages, 64 or 32 slots.
 template <int KP, bool STREAM>
 struct MmaCfg {
+  static constexpr bool dense = KP == 16 && !STREAM;
   static constexpr int tn = 64;
   static constexpr int nacc = 128 / tn;
-  static constexpr int stages = (KP == 16 && !STREAM) ? 1 : 2;
+  static constexpr int stages = dense ? 1 : 2;
   static constexpr int slots = KP == 16 ? 32 : 64;
-  static constexpr int min_blocks = (KP == 16 && !STREAM) ? 3 : 2;
+  static constexpr int groups = 1;
+  static constexpr int epi_warps = 4 * groups;
+  static constexpr int threads = 32 * (epi_warps + 2);
+  static constexpr int min_blocks = dense ? 3 : 2;
 };
 constexpr int kColBits = 13;        // low key bits holding the column in the leaf
 constexpr uint32_t kColMask = (1u << kColBits) - 1;
 constexpr int kMaxLeaf = 1 << kColBits;  // largest leaf the key can address
 constexpr int kCheck = 16;          // columns between flush checks
-constexpr int kEpiWarps = 4;
-constexpr int kMmaThreads = 32 * (kEpiWarps + 2);
 constexpr int kCentreRows = 64;     // rows averaged for a leaf's centre
 
 __device__ __forceinline__ bool before(float da, int32_t ia, float db, int32_t ib) {
@@ -470,11 +476,11 @@ constexpr int kSStages = 3;
 constexpr uint32_t kStreamA = kTM * 128, kStreamStage = kTM * 128 + kTN * 128;
 
 struct MmaSmem {
-  uint32_t a_off, b_off, buf_off, nrm_off, scl_off, bar_off, total;
+  uint32_t a_off, b_off, buf_off, nrm_off, scl_off, thr_off, bar_off, total;
 };
 
 __host__ __device__ inline MmaSmem mma_smem_layout(int kb, bool stream, int stages, int slots,
-                                                   int tn) {
+                                                   int tn, int groups) {
   MmaSmem L;
   L.a_off = 0;
   if (stream) {
@@ -484,9 +490,10 @@ __host__ __device__ inline MmaSmem mma_smem_layout(int kb, bool stream, int stag
     L.b_off = L.a_off + (uint32_t)kb * kTM * 128;
     L.buf_off = L.b_off + (uint32_t)stages * kb * tn * 128;
   }
-  L.nrm_off = L.buf_off + kTM * (uint32_t)slots * 4;
-  L.scl_off = L.nrm_off + kEpiWarps * (uint32_t)tn * 4;
-  L.bar_off = L.scl_off + kEpiWarps * (uint32_t)tn * 4;
+  L.nrm_off = L.buf_off + kTM * (uint32_t)slots * groups * 4;
+  L.scl_off = L.nrm_off + 4 * groups * (uint32_t)tn * 4;
+  L.thr_off = L.scl_off + 4 * groups * (uint32_t)tn * 4;
+  L.bar_off = L.thr_off + (uint32_t)groups * kTM * 4;
   L.total = L.bar_off + 24 * 8 + 16;
   return L;
 }
@@ -495,7 +502,8 @@ __host__ __device__ inline MmaSmem mma_smem_layout(int kb, bool stream, int stag
 // operands with per-row scales `scl` (scores are then scaled by the row's and
 // the column's scale); otherwise BF16.
 template <int KP, bool STREAM, bool FP8>
-__global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks)) k_leaf_mma(
+__global__ void __launch_bounds__(MmaCfg<KP, STREAM>::threads,
+                                  MmaCfg<KP, STREAM>::min_blocks) k_leaf_mma(
     const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
     const int32_t *__restrict__ goff, const int32_t *__restrict__ order,
     const float *__restrict__ nrm, const float *__restrict__ scl,
@@ -507,12 +515,14 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
   uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
   using Cfg = MmaCfg<KP, STREAM>;
   constexpr int kBufSlots = Cfg::slots;
-  constexpr int TN = Cfg::tn, NACC = Cfg::nacc;
+  constexpr int TN = Cfg::tn, NACC = Cfg::nacc, G = Cfg::groups, EPI = Cfg::epi_warps;
   static_assert(!STREAM || TN == kTN, "streamed stages hold kTN-column B blocks");
-  const MmaSmem L = mma_smem_layout(kb, STREAM, Cfg::stages, Cfg::slots, TN);
+  static_assert(NACC % G == 0, "a group owns whole accumulators");
+  const MmaSmem L = mma_smem_layout(kb, STREAM, Cfg::stages, Cfg::slots, TN, G);
   uint8_t *sA = smem + L.a_off;
   uint8_t *sB = smem + L.b_off;
-  uint32_t *buf = reinterpret_cast<uint32_t *>(smem + L.buf_off);  // [slot][row] keys
+  uint32_t *buf = reinterpret_cast<uint32_t *>(smem + L.buf_off);  // [group][slot][row] keys
+  float *thr_sh = reinterpret_cast<float *>(smem + L.thr_off);  // [group][row] KP-th best key
   float *nbuf = reinterpret_cast<float *>(smem + L.nrm_off);  // [warp][TN] column norms of a tile
   float *sbuf = reinterpret_cast<float *>(smem + L.scl_off);  // [warp][TN] column scales (FP8)
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L.bar_off);
@@ -547,13 +557,14 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
     }
     for (int b = 0; b < NACC; ++b) {
       mbar_init(acc_full + b, 1);
-      mbar_init(acc_empty + b, kEpiWarps * 32);
+      mbar_init(acc_empty + b, 4 * 32);  // the owning group's 128 threads
     }
     *abort_flag = 0;
     fence_barrier_init();
   }
-  if (warp == kEpiWarps + 1) tmem_alloc(tmem_slot, 128);  // NACC accumulators x TN columns
-  if (warp == kEpiWarps && lane == 0) {
+  for (int i = threadIdx.x; i < G * kTM; i += blockDim.x) thr_sh[i] = __int_as_float(0x7f800000);
+  if (warp == EPI + 1) tmem_alloc(tmem_slot, 128);  // NACC accumulators x TN columns
+  if (warp == EPI && lane == 0) {
     prefetch_tmap(&tmA);
     prefetch_tmap(&tmB);
   }
@@ -562,7 +573,7 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp == kEpiWarps) {
+  if (warp == EPI) {
     // ---- TMA producer
     if (lane == 0) {
       if constexpr (STREAM) {
@@ -596,7 +607,7 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
         }
       }
     }
-  } else if (warp == kEpiWarps + 1) {
+  } else if (warp == EPI + 1) {
     // ---- MMA issuer: 4 instructions per 128-byte K block (K = 16 BF16 or
     // 32 E4M3 values, 32 bytes each)
     if (lane == 0) {
@@ -654,8 +665,13 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
     // (conflict-free: consecutive rows are consecutive words); when any row
     // of the warp has too many pending, every row sorts its pending keys in
     // batches of 16 and merges them into its sorted list of KP keys with a
-    // bitonic network.
-    const int row = warp * 32 + lane;
+    // bitonic network.  With two groups, group g takes the column tiles
+    // c = g, g + 2, ... (accumulator g) and keeps its own list per row; each
+    // group filters with the smaller of the groups' KP-th best keys (a key
+    // above another group's KP-th best cannot be among the KP best of the
+    // union), and group 0 merges the lists at the end.
+    const int grp = warp / 4, wq = warp % 4;
+    const int row = wq * 32 + lane;
     const bool rvalid = r0 + row < m;
     float td[KP];
 #pragma unroll
@@ -680,7 +696,7 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
     // append chains) by a predicated shared-memory store, no branch; slot
     // addresses are 32-bit shared-window offsets.
     constexpr int kChains = 2, kLane = kBufSlots / kChains, kPerBatch = 16 / kChains;
-    uint32_t *const pbase = buf + row;
+    uint32_t *const pbase = buf + grp * kBufSlots * kTM + row;
     const uint32_t abase = smem_u32(pbase);
     uint32_t aslot[kChains];
 #pragma unroll
@@ -711,7 +727,15 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
       }
 #pragma unroll
       for (int q = 0; q < kChains; ++q) aslot[q] = abase + q * kLane * kTM * 4;
-      thr = fminf(thr0, td[KP - 1]);
+      float lim = td[KP - 1];
+      if constexpr (G > 1) {
+        volatile float *ts = thr_sh;
+        ts[grp * kTM + row] = lim;
+#pragma unroll
+        for (int g2 = 0; g2 < G; ++g2)
+          if (g2 != grp) lim = fminf(lim, ts[g2 * kTM + row]);
+      }
+      thr = fminf(thr0, lim);
     };
     // key = the score's high bits and the column bits of the packed norm
     // (one bit-select), stored only when the score beats the threshold
@@ -766,7 +790,7 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
         if (__any_sync(kFull, most > kLane - kCheck / kChains)) flush();
       }
     };
-    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t lane_base = tmem + ((uint32_t)(wq * 32) << 16);
     // column norms (and E4M3 scales) of a tile: lane l holds columns l and
     // l + 32, loaded one tile ahead; columns past the leaf carry an infinite
     // norm (a NaN once packed) and so never pass
@@ -781,8 +805,8 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
         if constexpr (FP8) ps[h] = in ? __ldg(scl + lo + col) : 0.0f;
       }
     };
-    load_cols(0);
-    for (int c = 0; c < nct; ++c) {
+    load_cols(grp);
+    for (int c = grp; c < nct; c += G) {
       const int b = c % NACC;
       // this tile's column norms, staged per warp (16-byte aligned reads)
       float *wn = nbuf + warp * TN;
@@ -799,7 +823,7 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
         if constexpr (FP8) ws[h * 32 + lane] = ps[h];
       }
       __syncwarp();
-      load_cols(c + 1);
+      load_cols(c + G);
       if (!__all_sync(kFull, mbar_wait(acc_full + b, (c / NACC) & 1))) {
         *abort_flag = 1;
         break;
@@ -815,7 +839,24 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
       mbar_arrive(acc_empty + b);
     }
     flush();
-    if (rvalid) {
+    if constexpr (G > 1) {
+      // groups g > 0 hand their sorted lists to group 0 through their own
+      // buffer slots (KP <= slots); a barrier over the epilogue warps only
+      if (grp > 0) {
+#pragma unroll
+        for (int j = 0; j < KP; ++j) pbase[j * kTM] = __float_as_uint(td[j]);
+      }
+      asm volatile("bar.sync 1, %0;" ::"n"(EPI * 32) : "memory");
+      if (grp == 0) {
+        for (int g2 = 1; g2 < G; ++g2) {
+          float sd[KP];
+#pragma unroll
+          for (int j = 0; j < KP; ++j) sd[j] = __uint_as_float(buf[(g2 * kBufSlots + j) * kTM + row]);
+          key_merge_into<KP, KP>(td, sd);
+        }
+      }
+    }
+    if (grp == 0 && rvalid) {
       // fold this tree's list into the running list: keys back to (squared
       // distance, point id); drop neighbours the running list already holds;
       // a bitonic merge keeps the KP best by (distance, id)
@@ -866,7 +907,7 @@ __global__ void __launch_bounds__(kMmaThreads, (MmaCfg<KP, STREAM>::min_blocks))
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == kEpiWarps + 1) {
+  if (warp == EPI + 1) {
     tc_fence_after();
     tmem_dealloc(tmem, 128);
   }
@@ -1151,7 +1192,7 @@ drpt_status mma_t(const MixedTreeArgs &a, const CUtensorMap &tmA, int kb, cudaSt
   using Cfg = MmaCfg<KP, STREAM>;
   CUtensorMap tmB;
   DRPT_TRY(make_tmap(&tmB, a.Xb, a.n, a.d_pad, Cfg::tn, a.fp8));
-  const MmaSmem L = mma_smem_layout(kb, STREAM, Cfg::stages, Cfg::slots, Cfg::tn);
+  const MmaSmem L = mma_smem_layout(kb, STREAM, Cfg::stages, Cfg::slots, Cfg::tn, Cfg::groups);
   const size_t smem = L.total + 1024;
   if (smem > 227 * 1024) {
     set_error("mixed leaf kernel: %zu bytes of shared memory needed", smem);
@@ -1160,7 +1201,7 @@ drpt_status mma_t(const MixedTreeArgs &a, const CUtensorMap &tmA, int kb, cudaSt
   const unsigned grid = (unsigned)(ceil_div(a.n, kTM) + a.nleaf);
   DRPT_CUDA(cudaFuncSetAttribute(k_leaf_mma<KP, STREAM, FP8>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_leaf_mma<KP, STREAM, FP8><<<grid, kMmaThreads, smem, s>>>(
+  k_leaf_mma<KP, STREAM, FP8><<<grid, Cfg::threads, smem, s>>>(
       tmA, tmB, a.goff, a.order, a.nrm, a.scl, a.tile_leaf, a.tile_r0, a.n_tiles, kb, a.tree,
       a.cand_idx, a.cand_dist, a.err);
   DRPT_LAUNCH_CHECK();
