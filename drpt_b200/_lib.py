@@ -52,6 +52,7 @@ class BuildDesc(ctypes.Structure):
         ("stream", ctypes.c_void_p), ("leaf_size", ctypes.c_int32), ("precision", ctypes.c_int32),
         ("learned_trees", ctypes.c_int32), ("learn_sample", ctypes.c_int32),
         ("learn_iters", ctypes.c_int32), ("locality", ctypes.c_int32),
+        ("list_width", ctypes.c_int32), ("reserved", ctypes.c_int32),
     ]
 
 
@@ -62,7 +63,7 @@ class BatchDesc(ctypes.Structure):
         ("precision", ctypes.c_int32), ("leaf_size", ctypes.c_int32), ("seed", ctypes.c_uint32),
         ("use_graph", ctypes.c_int32), ("density", ctypes.c_double),
         ("data_on_device", ctypes.c_int32), ("out_on_device", ctypes.c_int32),
-        ("stream", ctypes.c_void_p),
+        ("stream", ctypes.c_void_p), ("list_width", ctypes.c_int32), ("reserved", ctypes.c_int32),
     ]
 
 

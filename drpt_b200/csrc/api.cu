@@ -381,11 +381,18 @@ drpt_status leaf_depth(int64_t n, int leaf_size_in, int *gd_out) {
 // into oi / od.  Kernel launches only (no host synchronisation), so the
 // batched path can capture it in a CUDA graph; `timed` records the per-tree
 // events that the stats report.  mixed_check reads the kernels' error flag.
+// Candidates kept per point and tree (re-ranked at the end): the requested
+// width, or 16 for nn <= 10 and 32 otherwise; -1 when the request is not
+// 16 or 32 or is below nn.
+int list_width_of(int req, int nn) {
+  if (req == 0) return nn <= 10 ? 16 : 32;
+  return (req == 16 || req == 32) && req >= nn ? req : -1;
+}
+
 drpt_status mixed_leaf_phase(drpt_ctx *c, const void *X, int dtype, int64_t n, int d, int T,
-                             int nn, int fp8, const int32_t *order, const int32_t *goff,
+                             int nn, int kp, int fp8, const int32_t *order, const int32_t *goff,
                              int nleaf, int32_t *oi, float *od, bool timed, cudaStream_t s) {
   const int d_pad = mixed_d_pad(d, fp8);
-  const int kp = nn <= 10 ? 16 : 32;  // running candidates per point, re-ranked at the end
   cudaEvent_t *ev = c->ev;
   MixedTreeArgs a{};
   a.X = X;
@@ -637,7 +644,7 @@ drpt_status learn_and_project(drpt_ctx *c, const void *X, int dtype, int64_t n, 
   }
   DRPT_CUDA(cudaMemcpyAsync(iota_t, io.data(), io.size() * 4, cudaMemcpyHostToDevice, s));
   DRPT_CUDA(cudaMemcpyAsync(goff1, g2.data(), g2.size() * 4, cudaMemcpyHostToDevice, s));
-  DRPT_TRY(mixed_leaf_phase(c, xraw, DRPT_DTYPE_F32, S, d, 1, kLearnPairs, 0, iota_t, goff1, 1,
+  DRPT_TRY(mixed_leaf_phase(c, xraw, DRPT_DTYPE_F32, S, d, 1, kLearnPairs, 16, 0, iota_t, goff1, 1,
                             nbr_d, ndist, false, s));
   DRPT_TRY(mixed_check(c, s));
   std::vector<int32_t> nbr((size_t)S * kLearnPairs);
@@ -787,6 +794,11 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
     set_error("mixed mode supports nn <= 32 (got %d)", nn);
     return DRPT_ERR_UNSUPPORTED;
   }
+  const int kp = list_width_of(desc->list_width, nn);
+  if (kp < 0) {
+    set_error("list_width %d: 0, or 16 or 32 and at least nn = %d", desc->list_width, nn);
+    return DRPT_ERR_INVALID_ARG;
+  }
   if (desc->precision != DRPT_PRECISION_BF16 && desc->precision != DRPT_PRECISION_FP8_E4M3) {
     set_error("unknown precision %d", desc->precision);
     return DRPT_ERR_INVALID_ARG;
@@ -842,7 +854,7 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
   DRPT_TRY(global_trees(c, P, n, T, gd, 0, medians, &order, &goff, s));
   DRPT_CUDA(cudaEventRecord(ev[2], s));
 
-  DRPT_TRY(mixed_leaf_phase(c, X, desc->dtype, n, d, T, nn, fp8, order, goff, nleaf, oi, od,
+  DRPT_TRY(mixed_leaf_phase(c, X, desc->dtype, n, d, T, nn, kp, fp8, order, goff, nleaf, oi, od,
                             /*timed=*/true, s));
   DRPT_TRY(mixed_check(c, s));
   if (keep) {
@@ -1014,6 +1026,7 @@ drpt_status run_fp32_leaf(drpt_ctx *c, const drpt_build_desc *desc, const void *
 // every dataset's trees, leaves and lists equal its single build's.
 struct BatchPlan {
   int nsets = 0, l0 = 0, gdm = 0, nleaf = 0, T = 0, nn = 0, d = 0, dtype = 0, fp8 = 0, mode = 0;
+  int kp = 16;                   // mixed mode: candidates kept per point and tree
   int64_t n = 0;
   int ncols = 0;                 // T * (gdm - 1) projected columns
   CscDev csc{};
@@ -1036,6 +1049,7 @@ drpt_status batch_prepare(drpt_ctx *c, const drpt_batch_desc *desc, const int64_
   bp->nsets = nsets;
   bp->T = T;
   bp->nn = desc->nn;
+  bp->kp = list_width_of(desc->list_width, desc->nn);
   bp->d = d;
   bp->dtype = desc->dtype;
   bp->mode = desc->mode;
@@ -1134,7 +1148,7 @@ drpt_status batch_prepare(drpt_ctx *c, const drpt_batch_desc *desc, const int64_
   DRPT_TRY(ws_get(c, "lv_unit_lbase", Umax, &a.unit_lbase));
   DRPT_TRY(ws_get(c, "lv_node_nleft", Gmax, &a.node_nleft));
   if (bp->mode == DRPT_MODE_MIXED) {
-    const int d_pad = mixed_d_pad(d, bp->fp8), kp = bp->nn <= 10 ? 16 : 32;
+    const int d_pad = mixed_d_pad(d, bp->fp8), kp = bp->kp;
     const size_t tiles = (size_t)ceil_div(n, 128) + bp->nleaf;
     uint8_t *u8p;
     int32_t *i32p;
@@ -1211,7 +1225,7 @@ drpt_status batch_enqueue(drpt_ctx *c, const BatchPlan &bp, const void *X, int32
   }
   if (timed) DRPT_CUDA(cudaEventRecord(c->ev[2], s));
   if (bp.mode == DRPT_MODE_MIXED) {
-    DRPT_TRY(mixed_leaf_phase(c, X, bp.dtype, n, bp.d, T, bp.nn, bp.fp8, bp.order, bp.goff,
+    DRPT_TRY(mixed_leaf_phase(c, X, bp.dtype, n, bp.d, T, bp.nn, bp.kp, bp.fp8, bp.order, bp.goff,
                               bp.nleaf, oi, od, timed, s));
   } else {
     if (timed) DRPT_CUDA(cudaEventRecord(c->ev[3], s));
@@ -1320,6 +1334,10 @@ drpt_status drpt_build_graph_batched(drpt_ctx *c, const drpt_batch_desc *desc,
   if (desc->mode == DRPT_MODE_MIXED && (nn > 32 || d % 4 != 0 || d > 1024)) {
     set_error("mixed mode supports nn <= 32 and d %% 4 == 0, d <= 1024 (got nn %d, d %d)", nn, d);
     return DRPT_ERR_UNSUPPORTED;
+  }
+  if (desc->mode == DRPT_MODE_MIXED && list_width_of(desc->list_width, nn) < 0) {
+    set_error("list_width %d: 0, or 16 or 32 and at least nn = %d", desc->list_width, nn);
+    return DRPT_ERR_INVALID_ARG;
   }
   if (desc->use_graph && (!desc->data_on_device || !desc->out_on_device)) {
     set_error("graph mode needs device input and output pointers");

@@ -63,7 +63,7 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
                 density: float = 0.0, local_seeds=None, device: int = 0, stream=None,
                 out=None, leaf_size: int = 0, precision: str = "bf16", learned_trees: int = 0,
                 learn_sample: int = 0, learn_iters: int = 0, locality: bool = False,
-                _index_out=None):
+                list_width: int = 0, _index_out=None):
     """k-NN graph of `data` (n x d, uint8 or float32; a NumPy array in host
     memory or a CUDA tensor).  Returns (idx, dist, stats): idx int32 and dist
     float32 of shape (n, nn), each point's nn nearest distinct neighbours other
@@ -75,7 +75,9 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
     on a sample of `learn_sample` points (0 = 8,192) with `learn_iters` Adam
     steps per level (0 = 10).  `locality` (exact and fast modes) runs the
     reference's locality relabelling of the global leaves; at one rank the
-    graph is the same either way."""
+    graph is the same either way.  `list_width` (mixed mode: 16 or 32, at
+    least nn; 0 = 16 for nn <= 10, else 32) is how many candidates per point
+    and tree the mixed form keeps for its final FP32 re-rank."""
     on_dev = _is_cuda_tensor(data)
     if not on_dev:
         data = np.ascontiguousarray(data)
@@ -99,6 +101,7 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
     desc.learned_trees, desc.learn_sample = learned_trees, learn_sample
     desc.learn_iters = learn_iters
     desc.locality = 1 if locality else 0
+    desc.list_width = list_width
     desc.data_on_device = 1 if on_dev else 0
     desc.out_on_device = desc.data_on_device
     if on_dev:
@@ -190,7 +193,7 @@ def build_index(data, ntrees: int, nn: int, seed: int, **kw):
 
 def build_graph_batched(data, offsets, ntrees: int, nn: int, seed: int, *, mode: str = "mixed",
                         leaf_size: int = 0, precision: str = "bf16", density: float = 0.0,
-                        use_graph: bool = False, stream=None, out=None):
+                        use_graph: bool = False, stream=None, out=None, list_width: int = 0):
     """k-NN graphs of many independent datasets in one call
     (drpt_build_graph_batched).  `data` holds the datasets row after row (a
     NumPy array or a CUDA tensor, uint8 or float32); dataset s is rows
@@ -198,7 +201,7 @@ def build_graph_batched(data, offsets, ntrees: int, nn: int, seed: int, *, mode:
     each dataset's first row; each dataset's rows equal build_graph on that
     dataset alone.  `use_graph` captures the device work in a CUDA graph and
     replays it on later calls with the same offsets, parameters and tensors
-    (CUDA tensors only)."""
+    (CUDA tensors only).  `list_width` as in build_graph."""
     offs = np.ascontiguousarray(np.asarray(offsets, dtype=np.int64))
     on_dev = _is_cuda_tensor(data)
     data = data.contiguous() if on_dev else np.ascontiguousarray(data)
@@ -210,6 +213,7 @@ def build_graph_batched(data, offsets, ntrees: int, nn: int, seed: int, *, mode:
     desc.ntrees, desc.nn = ntrees, nn
     desc.mode = {"mixed": _lib.MODE_MIXED, "fp32_leaf": _lib.MODE_FP32_LEAF}[mode]
     desc.precision = {"bf16": _lib.PRECISION_BF16, "fp8": _lib.PRECISION_FP8_E4M3}[precision]
+    desc.list_width = list_width
     desc.leaf_size, desc.seed, desc.density = leaf_size, seed & 0xFFFFFFFF, density
     desc.use_graph = 1 if use_graph else 0
     desc.data_on_device = desc.out_on_device = 1 if on_dev else 0

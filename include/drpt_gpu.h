@@ -116,6 +116,10 @@ typedef struct {
                                  relabelling (-locality 1) between the global
                                  and the local trees; at one rank it only
                                  renumbers global leaves, the graph is the same */
+  int32_t list_width;         /* mixed mode: candidates kept per point and tree
+                                 for the final re-rank, 16 or 32 and >= nn
+                                 (0 = 16 for nn <= 10, else 32) */
+  int32_t reserved;
 } drpt_build_desc;
 
 typedef struct {
@@ -183,6 +187,8 @@ typedef struct {
   int32_t data_on_device;     /* 1: data is device memory */
   int32_t out_on_device;      /* 1: outputs are device memory */
   void *stream;               /* cudaStream_t; NULL = legacy default */
+  int32_t list_width;         /* mixed mode: as drpt_build_desc.list_width */
+  int32_t reserved;
 } drpt_batch_desc;
 
 /* Builds every dataset of the batch together: one projection launch, one
