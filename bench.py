@@ -336,9 +336,13 @@ def other_workload(args):
         idx = torch.empty((n, nn), dtype=torch.int32, device="cuda")
         dst = torch.empty((n, nn), dtype=torch.float32, device="cuda")
 
-        def run(mode="mixed", trees=T, precision=prec, learned=lt, out=(idx, dst)):
+        # config 5 trains the split MLPs on a 50k-point sample
+        sample = 50_000 if lt else 0
+
+        def run(mode="mixed", trees=T, precision=prec, learned=lt, out=(idx, dst), smp=sample):
             return build_graph(Xd, trees, nn, SEED_PROJ, mode=mode, leaf_size=leaf,
-                               precision=precision, learned_trees=learned, out=out)[2]
+                               precision=precision, learned_trees=learned, out=out,
+                               learn_sample=smp if learned else 0)[2]
         for _ in range(warm):
             run()
         with ClockSampler(0) as clocks:
@@ -361,7 +365,8 @@ def other_workload(args):
         if wl == "fbin-2m-960":
             others.append(("mixed_bf16", dict(precision="bf16")))
         if lt:
-            others += [(f"mixed_{T}_random_trees", dict(learned=0)),
+            others += [("mixed_learned_sample_8192", dict(smp=8192)),
+                       (f"mixed_{T}_random_trees", dict(learned=0)),
                        (f"mixed_{2 * T}_random_trees", dict(trees=2 * T, learned=0)),
                        (f"fp32_leaf_{2 * T}_random_trees", dict(mode="fp32_leaf", trees=2 * T,
                                                                   learned=0))]

@@ -533,6 +533,8 @@ drpt_status mixed_check(drpt_ctx *c, cudaStream_t s) {
 // as on a random projection.
 constexpr int kLearnIters = 10;      // default Adam steps per level
 constexpr int kLearnSample = 8192;   // default sample size
+constexpr int kLearnSampleMax = 1 << 20;
+constexpr int kPairLeaf = 8192;      // largest leaf of the sample's neighbour search
 constexpr float kLearnLr = 0.01f;
 constexpr int kLearnPairs = 10;      // neighbours per sample point
 constexpr int kLearnChunks = 64;     // row chunks of the backward pass
@@ -644,8 +646,40 @@ drpt_status learn_and_project(drpt_ctx *c, const void *X, int dtype, int64_t n, 
   }
   DRPT_CUDA(cudaMemcpyAsync(iota_t, io.data(), io.size() * 4, cudaMemcpyHostToDevice, s));
   DRPT_CUDA(cudaMemcpyAsync(goff1, g2.data(), g2.size() * 4, cudaMemcpyHostToDevice, s));
-  DRPT_TRY(mixed_leaf_phase(c, xraw, DRPT_DTYPE_F32, S, d, 1, kLearnPairs, 16, 0, iota_t, goff1, 1,
-                            nbr_d, ndist, false, s));
+  // The brute force runs over leaves of at most kPairLeaf points (the leaf
+  // kernel's limit): a larger sample is sorted along a seeded random
+  // direction and cut into equal consecutive chunks, a one-level tree.
+  const int chunks = (S + kPairLeaf - 1) / kPairLeaf;
+  const int32_t *pord = iota_t, *poff = goff1;
+  if (chunks > 1) {
+    std::vector<float> hx((size_t)S * d);
+    DRPT_CUDA(cudaMemcpyAsync(hx.data(), xraw, hx.size() * 4, cudaMemcpyDeviceToHost, s));
+    DRPT_CUDA(cudaStreamSynchronize(s));
+    std::mt19937 dg(seed ^ 0x2545f491u);
+    std::normal_distribution<float> nd(0.0f, 1.0f);
+    std::vector<float> w(d);
+    for (int k = 0; k < d; ++k) w[k] = nd(dg);
+    std::vector<double> key(S);
+    for (int i = 0; i < S; ++i) {
+      double acc = 0.0;
+      for (int k = 0; k < d; ++k) acc += (double)hx[(size_t)i * d + k] * w[k];
+      key[i] = acc;
+    }
+    std::vector<int32_t> po(S), pf(chunks + 1);
+    for (int i = 0; i < S; ++i) po[i] = i;
+    std::stable_sort(po.begin(), po.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+    for (int q = 0; q <= chunks; ++q) pf[q] = (int32_t)((int64_t)S * q / chunks);
+    int32_t *dpo, *dpf;
+    DRPT_TRY(ws_get(c, "ln_pair_order", (size_t)S, &dpo));
+    DRPT_TRY(ws_get(c, "ln_pair_off", (size_t)chunks + 1, &dpf));
+    DRPT_CUDA(cudaMemcpyAsync(dpo, po.data(), po.size() * 4, cudaMemcpyHostToDevice, s));
+    DRPT_CUDA(cudaMemcpyAsync(dpf, pf.data(), pf.size() * 4, cudaMemcpyHostToDevice, s));
+    DRPT_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
+    pord = dpo;
+    poff = dpf;
+  }
+  DRPT_TRY(mixed_leaf_phase(c, xraw, DRPT_DTYPE_F32, S, d, 1, kLearnPairs, 16, 0, pord, poff,
+                            chunks, nbr_d, ndist, false, s));
   DRPT_TRY(mixed_check(c, s));
   std::vector<int32_t> nbr((size_t)S * kLearnPairs);
   DRPT_CUDA(cudaMemcpy(nbr.data(), nbr_d, nbr.size() * 4, cudaMemcpyDeviceToHost));
@@ -809,7 +843,8 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
     return DRPT_ERR_UNSUPPORTED;
   }
   const int learned = desc->learned_trees;
-  if (learned < 0 || learned > T || desc->learn_sample < 0 || desc->learn_iters < 0) {
+  if (learned < 0 || learned > T || desc->learn_sample < 0 || desc->learn_sample > kLearnSampleMax ||
+      desc->learn_iters < 0) {
     set_error("learned_trees %d (of %d), learn_sample %d or learn_iters %d out of range", learned,
               T, desc->learn_sample, desc->learn_iters);
     return DRPT_ERR_INVALID_ARG;

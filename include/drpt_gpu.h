@@ -110,7 +110,10 @@ typedef struct {
                                  ones) split on learned MLP values instead of
                                  random projections (0 = none; d <= 256) */
   int32_t learn_sample;       /* sample points the split MLPs train on
-                                 (0 = 8,192) */
+                                 (0 = 8,192; at most 2^20; a sample above
+                                 8,192 finds its neighbour pairs in chunks of
+                                 at most 8,192 points sorted along a random
+                                 direction) */
   int32_t learn_iters;        /* Adam steps per level (0 = 10) */
   int32_t locality;           /* exact and fast modes: 1 runs the locality
                                  relabelling (-locality 1) between the global

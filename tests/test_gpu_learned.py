@@ -99,3 +99,25 @@ def test_learned_argument_checks(torch):
     with pytest.raises(DrptError) as e:
         build_graph(X, 2, 10, 1, mode="mixed", learned_trees=1)
     assert e.value.status == 8
+
+
+def test_large_sample_trains_in_chunks(torch, manifold):
+    """A sample above the leaf kernel's 8,192-point limit finds its
+    neighbour pairs in chunks; training still lowers the loss, the build is
+    deterministic and keeps the gain over random trees; samples beyond
+    2^20 are rejected."""
+    X, Xd, q, ti = manifold
+    a = build_graph(Xd, 8, 10, 12345, mode="mixed", leaf_size=1024, learned_trees=8,
+                    learn_sample=30_000)
+    b = build_graph(Xd, 8, 10, 12345, mode="mixed", leaf_size=1024, learned_trees=8,
+                    learn_sample=30_000)
+    torch.cuda.synchronize()
+    assert torch.equal(a[0], b[0])
+    st = a[2]
+    assert st.learn_loss_end < 0.8 * st.learn_loss_start, st.as_dict()
+    r0, _, _ = build_graph(Xd, 8, 10, 12345, mode="mixed", leaf_size=1024)
+    assert (recall.recall_at_k(a[0].cpu().numpy()[q], ti)
+            >= recall.recall_at_k(r0.cpu().numpy()[q], ti) + 0.08)
+    with pytest.raises(DrptError) as e:
+        build_graph(Xd, 4, 10, 1, mode="mixed", learned_trees=2, learn_sample=(1 << 20) + 1)
+    assert e.value.status == 1
