@@ -127,9 +127,11 @@ drpt_status geometry(int64_t n, int tree_depth, double ratio, Geometry *g) {
 }
 
 // K1 with the CSC of the used columns of B built on the host.
+// `tag` names the workspace buffers of the CSC ("csc": the build's own,
+// which an index keeps).
 drpt_status project_cols(drpt_ctx *c, const void *X, int dtype, int64_t n, int d, const float *B,
                          int L, const std::vector<int32_t> &cols, float *P, cudaStream_t s,
-                         int *nnz_out = nullptr) {
+                         int *nnz_out = nullptr, const char *tag = "csc") {
   const int ncols = (int)cols.size();
   std::vector<int32_t> colptr(ncols + 1, 0), row;
   std::vector<float> val;
@@ -145,9 +147,10 @@ drpt_status project_cols(drpt_ctx *c, const void *X, int dtype, int64_t n, int d
   }
   int32_t *dcol, *drow;
   float *dval;
-  DRPT_TRY(ws_get(c, "csc_colptr", colptr.size(), &dcol));
-  DRPT_TRY(ws_get(c, "csc_row", std::max<size_t>(row.size(), 1), &drow));
-  DRPT_TRY(ws_get(c, "csc_val", std::max<size_t>(val.size(), 1), &dval));
+  const std::string t(tag);
+  DRPT_TRY(ws_get(c, (t + "_colptr").c_str(), colptr.size(), &dcol));
+  DRPT_TRY(ws_get(c, (t + "_row").c_str(), std::max<size_t>(row.size(), 1), &drow));
+  DRPT_TRY(ws_get(c, (t + "_val").c_str(), std::max<size_t>(val.size(), 1), &dval));
   // Pageable sources: the copies complete before these calls return.
   DRPT_CUDA(cudaMemcpyAsync(dcol, colptr.data(), colptr.size() * 4, cudaMemcpyHostToDevice, s));
   if (!row.empty()) {
@@ -652,19 +655,18 @@ drpt_status learn_and_project(drpt_ctx *c, const void *X, int dtype, int64_t n, 
   const int chunks = (S + kPairLeaf - 1) / kPairLeaf;
   const int32_t *pord = iota_t, *poff = goff1;
   if (chunks > 1) {
-    std::vector<float> hx((size_t)S * d);
-    DRPT_CUDA(cudaMemcpyAsync(hx.data(), xraw, hx.size() * 4, cudaMemcpyDeviceToHost, s));
-    DRPT_CUDA(cudaStreamSynchronize(s));
+    // the sample projected on the GPU onto one seeded Gaussian direction
     std::mt19937 dg(seed ^ 0x2545f491u);
     std::normal_distribution<float> nd(0.0f, 1.0f);
     std::vector<float> w(d);
     for (int k = 0; k < d; ++k) w[k] = nd(dg);
-    std::vector<double> key(S);
-    for (int i = 0; i < S; ++i) {
-      double acc = 0.0;
-      for (int k = 0; k < d; ++k) acc += (double)hx[(size_t)i * d + k] * w[k];
-      key[i] = acc;
-    }
+    float *dkey;
+    DRPT_TRY(ws_get(c, "ln_pair_key", (size_t)S, &dkey));
+    DRPT_TRY(project_cols(c, xraw, DRPT_DTYPE_F32, S, d, w.data(), 1, std::vector<int32_t>{0},
+                          dkey, s, nullptr, "ln_pair_csc"));
+    std::vector<float> key(S);
+    DRPT_CUDA(cudaMemcpyAsync(key.data(), dkey, (size_t)S * 4, cudaMemcpyDeviceToHost, s));
+    DRPT_CUDA(cudaStreamSynchronize(s));
     std::vector<int32_t> po(S), pf(chunks + 1);
     for (int i = 0; i < S; ++i) po[i] = i;
     std::stable_sort(po.begin(), po.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });

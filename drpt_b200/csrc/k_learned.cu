@@ -428,20 +428,44 @@ __global__ void k_stack(const float *__restrict__ params, int T, int d, int np, 
 
 // Per-dimension mean of the sample rows and the scalar scale
 // 1 / sqrt(mean over dimensions of the variance), FP64 in fixed order.
-__global__ void k_sample_mean(const float *__restrict__ Xr, int S, int d, float *__restrict__ c,
-                              double *__restrict__ var) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= d) return;
+// Block: 32 dimensions (lane tx) x 8 row phases (ty): thread (tx, ty) adds
+// rows ty, ty + 8, ... of dimension k0 + tx in order (coalesced 128-byte row
+// pieces per warp), the 8 phase sums are added in phase order; the squared
+// deviations from the mean follow in a second pass.
+__global__ void __launch_bounds__(256) k_sample_mean(const float *__restrict__ Xr, int S, int d,
+                                                     float *__restrict__ c,
+                                                     double *__restrict__ var) {
+  __shared__ double part[8][32];
+  __shared__ double mean[32];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int k = blockIdx.x * 32 + tx;
   double s = 0.0;
-  for (int i = 0; i < S; ++i) s += Xr[(int64_t)i * d + k];
-  const double m = s / S;
-  double q = 0.0;
-  for (int i = 0; i < S; ++i) {
-    const double df = Xr[(int64_t)i * d + k] - m;
-    q += df * df;
+  if (k < d)
+    for (int i = ty; i < S; i += 8) s += Xr[(int64_t)i * d + k];
+  part[ty][tx] = s;
+  __syncthreads();
+  if (ty == 0) {
+    double t = 0.0;
+    for (int p = 0; p < 8; ++p) t += part[p][tx];
+    mean[tx] = t / S;
   }
-  c[k] = (float)m;
-  var[k] = q / S;
+  __syncthreads();
+  const double m = mean[tx];
+  double q = 0.0;
+  if (k < d)
+    for (int i = ty; i < S; i += 8) {
+      const double df = Xr[(int64_t)i * d + k] - m;
+      q += df * df;
+    }
+  __syncthreads();  // part is reused
+  part[ty][tx] = q;
+  __syncthreads();
+  if (ty == 0 && k < d) {
+    double t = 0.0;
+    for (int p = 0; p < 8; ++p) t += part[p][tx];
+    c[k] = (float)m;
+    var[k] = t / S;
+  }
 }
 
 __global__ void k_sample_scale(const double *__restrict__ var, int d, float *__restrict__ inv_sigma) {
@@ -701,7 +725,7 @@ drpt_status launch_stack(const LearnArgs &a, int d_pad, int levels, int level,
 
 drpt_status launch_sample_scale(const float *Xr, int S, int d, float *c, double *var,
                                 float *inv_sigma, cudaStream_t s) {
-  k_sample_mean<<<(unsigned)ceil_div(d, 128), 128, 0, s>>>(Xr, S, d, c, var);
+  k_sample_mean<<<(unsigned)ceil_div(d, 32), 256, 0, s>>>(Xr, S, d, c, var);
   k_sample_scale<<<1, 32, 0, s>>>(var, d, inv_sigma);
   DRPT_LAUNCH_CHECK();
   return DRPT_OK;

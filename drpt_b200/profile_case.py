@@ -32,6 +32,7 @@ def main() -> None:
     ap.add_argument("--leaf", type=int, default=0, help="mixed mode: target leaf size")
     ap.add_argument("--precision", default="bf16", choices=["bf16", "fp8"])
     ap.add_argument("--learned", type=int, default=0, help="mixed mode: learned trees")
+    ap.add_argument("--learn-sample", type=int, default=0, help="learned trees: sample size")
     ap.add_argument("--data", default="clustered", choices=["clustered", "anisotropic", "manifold"])
     args = ap.parse_args()
     if args.data == "clustered":
@@ -43,7 +44,8 @@ def main() -> None:
     Xd = torch.from_numpy(X).cuda()
     for _ in range(args.reps):
         _, _, st = build_graph(Xd, args.trees, args.nn, 12345, mode=args.mode, leaf_size=args.leaf,
-                               precision=args.precision, learned_trees=args.learned)
+                               precision=args.precision, learned_trees=args.learned,
+                               learn_sample=args.learn_sample)
     torch.cuda.synchronize()
     print({k: round(v, 3) if isinstance(v, float) else v for k, v in st.as_dict().items()})
 
