@@ -57,3 +57,16 @@ def test_list_width(torch):
     with pytest.raises(DrptError) as e:  # 16 keys cannot hold 20 neighbours
         build_graph(X, 4, 20, 5, mode="mixed", leaf_size=512, list_width=16)
     assert e.value.status == 1
+
+
+def test_tune_graph_picks_a_measured_setting(torch):
+    X = torch.from_numpy(synth.clustered_f32(60_000, 32, n_clusters=60, seed=8)).cuda()
+    r = autotune.tune_graph(X, 4, 10, 2, leaf_sizes=(512, 1024), reps=1, queries=200)
+    assert len(r["trials"]) == 4 and not r["cached"]
+    assert autotune.choose(r["trials"], 0.90) == min(
+        [t for t in r["trials"] if t["recall"] >= 0.90] or [max(r["trials"],
+                                                               key=lambda t: t["recall"])],
+        key=lambda t: t["ms"])
+    i1, d1, _ = build_graph(X, 4, 10, 2, mode="mixed", leaf_size=r["leaf_size"],
+                            list_width=r["list_width"])
+    assert i1.shape == (60_000, 10) and (i1 >= 0).all()
