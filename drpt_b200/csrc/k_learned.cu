@@ -226,7 +226,9 @@ __global__ void k_point_grad(const float *__restrict__ f, int S, const int32_t *
 // ------------------------------------------------------------------ L6
 // Block (row chunk, tree, 128-dimension tile): partial dW1 over the chunk's
 // rows for 64 units x 128 dimensions (thread (ty, tx): units 4ty..4ty+3,
-// dimensions 8tx..8tx+7), rows in steps of 32 through shared memory.
+// dimensions 4tx..4tx+3 and 64+4tx..64+4tx+3, so that the 16 lanes' float4
+// reads of a row cover 64 consecutive floats: no bank conflicts), rows in
+// steps of 32 through shared memory.
 // Dimension tile 0 also writes the partials of b1, w2 and b2.  Partials:
 // T x R x np.
 __global__ void __launch_bounds__(256) k_mlp_bwd(const float *__restrict__ Xs, int S, int d,
@@ -266,8 +268,8 @@ __global__ void __launch_bounds__(256) k_mlp_bwd(const float *__restrict__ Xs, i
 #pragma unroll 4
     for (int q = 0; q < 32; ++q) {
       const float4 z = *reinterpret_cast<const float4 *>(&dz[q][4 * ty]);
-      const float4 x0 = *reinterpret_cast<const float4 *>(&xs[q][8 * tx]);
-      const float4 x1 = *reinterpret_cast<const float4 *>(&xs[q][8 * tx + 4]);
+      const float4 x0 = *reinterpret_cast<const float4 *>(&xs[q][4 * tx]);
+      const float4 x1 = *reinterpret_cast<const float4 *>(&xs[q][64 + 4 * tx]);
       const float zv[4] = {z.x, z.y, z.z, z.w};
       const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
 #pragma unroll
@@ -290,7 +292,7 @@ __global__ void __launch_bounds__(256) k_mlp_bwd(const float *__restrict__ Xs, i
   for (int u = 0; u < 4; ++u)
 #pragma unroll
     for (int v = 0; v < 8; ++v) {
-      const int h = 4 * ty + u, k = k0 + 8 * tx + v;
+      const int h = 4 * ty + u, k = k0 + (v < 4 ? 4 * tx + v : 64 + 4 * tx + v - 4);
       if (k < d) out[(int64_t)h * d + k] = acc[u][v];
     }
   if (blockIdx.z == 0 && threadIdx.x < kH) {
