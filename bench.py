@@ -61,8 +61,12 @@ MIXED_TREES, MIXED_LEAF = 6, 1024   # mixed form: trees and target global-leaf s
 PLAIN_MATCH_TREES = 384             # the reference method with many more trees
 SEED_PROJ = 12345
 CPU_SAMPLE = 32_768  # bounded sample for the CPU baseline (about 10-30 s of CPU work)
-REF_STEP_SAMPLE = 16_384  # per timed step of --impl reference
-REF_WARMUP_SAMPLE = 4_096  # per untimed warm-up step of --impl reference
+# Samples of --impl reference, timed and untimed steps: the size of the CPU
+# baseline's sample.  On some smaller samples of this distribution (4,096,
+# 8,192 and 16,384 points among them) the reference's smallest global leaf is
+# too small for its local trees and it throws std::out_of_range.
+REF_STEP_SAMPLE = 32_768
+REF_WARMUP_SAMPLE = 32_768
 WORKLOAD = ("1,000,000 x 128 float32 (fbin-shaped), 1000 Gaussian clusters, centres U[0,200]^128, "
             "sigma 12, clipped to [0,255]; nn=10; plain form ntrees=16 (reference parameters)")
 
