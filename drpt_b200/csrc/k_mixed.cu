@@ -14,8 +14,8 @@
 //                       of the rounded row
 //   K9  k_tile_plan     row tiles of 128 points of every leaf
 //   K10 k_leaf_mma      per row tile: TMA-fed tcgen05 MMAs (BF16 x BF16 ->
-//                       FP32 in Tensor Memory, M = 128 rows, N = 32 or 64
-//                       columns per tile, K = the padded dimension), epilogue scores
+//                       FP32 in Tensor Memory, M = 128 rows, N = 64 columns
+//                       per tile, K = the padded dimension), epilogue scores
 //                       ||y||^2 - 2 x.y per column and keeps each row's KP
 //                       best in registers (threshold filter seeded from the
 //                       running list, per-thread shared-memory buffer,
