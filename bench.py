@@ -622,7 +622,8 @@ def main():
         "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e,
         "gpu_launches": launches,
     }
-    print(json.dumps(line), flush=True)
+    if rank == 0:  # one line per job; every rank's timing is already max-reduced
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
