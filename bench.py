@@ -68,7 +68,25 @@ CPU_SAMPLE = 32_768  # bounded sample for the CPU baseline (about 10-30 s of CPU
 REF_STEP_SAMPLE = 32_768
 REF_WARMUP_SAMPLE = 32_768
 WORKLOAD = ("1,000,000 x 128 float32 (fbin-shaped), 1000 Gaussian clusters, centres U[0,200]^128, "
-            "sigma 12, clipped to [0,255]; nn=10; plain form ntrees=16 (reference parameters)")
+            "sigma 12, clipped to [0,255]; nn=10")
+# Tree parameters of each arm.  The metric is points/s at recall@10 >= 0.90:
+# the mixed form's trees are chosen for that recall.  The reference's own
+# parameters (16 trees, positional local split) give a recall that depends on
+# its thread count: at one thread every node lists its points in index order
+# and the positional chunks of all trees repeat the same neighbours (recall@10
+# 0.55 on the 32,768-point sample, 0.10 at 1M points, the order the exact
+# form reproduces); with many threads the order inside a node varies per tree
+# and recall rises (0.96 on the same sample at 8 threads).  The reference arm
+# reports the recall of the run it timed.
+TREES_MIXED = (f"mixed form: {MIXED_TREES} trees, global leaves of about {MIXED_LEAF} points "
+               "brute-forced whole (chosen for recall@10 >= 0.90)")
+TREES_REFERENCE = (f"reference parameters: {NTREES} trees, tree depth int(log2 n - 2), ratio 0.6, "
+                   "positional local split")
+# The reference's cblas calls (sgemm of the projection, saxpy/snrm2 of its
+# distance) run in the project's ordered cblas (plain loops in a fixed
+# summation order, oracle/refbuild/cblas_ordered.cpp): the host has no
+# OpenBLAS, the library the reference's CMake file names.
+REF_CBLAS = "ordered cblas (plain loops, oracle/refbuild/cblas_ordered.cpp); no OpenBLAS on the host"
 
 
 def _env_int(name, default):
@@ -153,14 +171,17 @@ def _reference_sample(tmpdir: str, n: int):
     return X, path
 
 
-def run_reference_once(path: str, n: int, threads: int):
-    """One run of the reference binary; returns (build_s, query_s, kind)."""
+def run_reference_once(path: str, n: int, threads: int, dump: str | None = None):
+    """One run of the reference binary; returns (build_s, query_s, kind).
+    `dump`: a file for its merged neighbour lists (written after the timed
+    phases)."""
     ref = os.path.join(ROOT, "oracle", "_ref", "drpt_ref")
     seeds = ",".join(str(s) for s in [SEED_PROJ] + list(range(1, NTREES + 1)))
     if os.path.exists(ref):
         out_dir = tempfile.mkdtemp()
         cmd = (f"ulimit -s unlimited; exec {ref} -input {path} -output {out_dir}/ -data-set-size {n} "
-               f"-dimension {DIM} -ntrees {NTREES} -nn {NN} -locality 0 -data-file-format 1 -no-write")
+               f"-dimension {DIM} -ntrees {NTREES} -nn {NN} -locality 0 -data-file-format 1 -no-write"
+               + (f" -dump {dump}" if dump else ""))
         env = dict(os.environ, DRPT_REF_SEEDS=seeds, OMP_NUM_THREADS=str(threads),
                    OMP_PROC_BIND="true")
         r = subprocess.run(["bash", "-c", cmd], env=env, capture_output=True, text=True)
@@ -182,16 +203,34 @@ def run_reference_once(path: str, n: int, threads: int):
     return t1 - t0, 0.0, "port"
 
 
+def reference_recall(X, dump: str, queries: int = 1000) -> float:
+    """recall@10 of the reference's merged lists (each point's first nn = 10
+    non-self candidates; the edge list it writes holds the first 9) against
+    FP64 exact neighbours of a seeded sample, by the CPU checker."""
+    import oracle
+    from oracle import refdump
+    from drpt_b200 import recall
+    lists = refdump.read(dump)["lists"]
+    n = len(X)
+    idx, _ = refdump.first_k_non_self(lists, n, NN)
+    q = recall.sample_queries(n, queries, seed=7)
+    ti, _ = oracle.exact_knn(X, q, NN)
+    return recall.recall_at_k(idx[q], ti)
+
+
 def cpu_baseline(n: int = CPU_SAMPLE):
     threads = _cores()
     with tempfile.TemporaryDirectory() as tmp:
-        _, path = _reference_sample(tmp, n)
-        b, q, kind = run_reference_once(path, n, threads)
+        X, path = _reference_sample(tmp, n)
+        dump = os.path.join(tmp, "lists.bin")
+        b, q, kind = run_reference_once(path, n, threads, dump=dump)
+        rec = reference_recall(X, dump) if kind == "reference" else None
     return {"value": n / (b + q), "unit": "points/s", "cores": threads if kind == "reference" else 1,
             "kind": kind,
             "sample": f"{n} points of the same distribution (clusters scaled to {max(1, round(N_CLUSTERS * n / N_POINTS))}), "
-                      f"ntrees={NTREES}, nn={NN}, 1 rank x {threads if kind == 'reference' else 1} threads; "
-                      f"time = index building + querying ({b:.2f} s + {q:.2f} s)"}
+                      f"{TREES_REFERENCE}, nn={NN}, 1 rank x {threads if kind == 'reference' else 1} threads; "
+                      f"time = index building + querying ({b:.2f} s + {q:.2f} s); {REF_CBLAS}",
+            "recall@10": rec}
 
 
 def reference_arm(args):
@@ -200,15 +239,21 @@ def reference_arm(args):
         return
     threads = _cores()
     times = []
+    rec = None
     with tempfile.TemporaryDirectory() as tmp:
         _, wpath = _reference_sample(tmp, REF_WARMUP_SAMPLE)
         for _ in range(args.warmup):
             run_reference_once(wpath, REF_WARMUP_SAMPLE, threads)
-        _, path = _reference_sample(tmp, REF_STEP_SAMPLE)
+        X, path = _reference_sample(tmp, REF_STEP_SAMPLE)
         kind = "reference"
         for _ in range(args.steps):
             b, q, kind = run_reference_once(path, REF_STEP_SAMPLE, threads)
             times.append(b + q)
+        if kind == "reference":
+            # quality of what was timed: one more untimed run dumps its lists
+            dump = os.path.join(tmp, "lists.bin")
+            run_reference_once(path, REF_STEP_SAMPLE, threads, dump=dump)
+            rec = reference_recall(X, dump)
     sec = sum(times) / len(times)
     value = REF_STEP_SAMPLE / sec
     line = {
@@ -216,8 +261,12 @@ def reference_arm(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_points": REF_STEP_SAMPLE, "ranks": 1,
-                   "threads": threads},
+        "config": {"workload": WORKLOAD, "trees": TREES_REFERENCE, "ntrees": NTREES,
+                   "sample_points": REF_STEP_SAMPLE, "ranks": 1, "threads": threads,
+                   "recall@10": rec, "recall_sample": 1000, "cblas": REF_CBLAS,
+                   "note": "the sample is bounded so that the run ends in minutes; the "
+                           "reference's recall depends on its thread count (the order of "
+                           "points inside a node feeds its positional local split)"},
         "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads if kind == "reference" else 1,
                          "kind": kind,
                          "sample": f"{REF_STEP_SAMPLE} points of the same distribution per timed step "
@@ -388,19 +437,21 @@ def other_workload(args):
         mma_ms = st.ms_leaf_mma / T
         flops = 2.0 * d * st.sum_leaf_sq / T
         fp8 = prec == "fp8"
-        peak = peaks.get("bf16_tflops_sustained", 1414.3) * (2 if fp8 else 1)
+        peak = peaks.get("bf16_tflops", 1590.0) * (2 if fp8 else 1)
         roof = {"kernel": f"k_leaf_mma ({'E4M3' if fp8 else 'BF16'} tcgen05 Gram tiles + top-k "
                           "epilogue), per launch",
                 "bound": "tensor", "achieved": flops / (mma_ms * 1e-3) / 1e12, "peak": peak,
                 "unit": "TFLOP/s", "frac": flops / (mma_ms * 1e-3) / 1e12 / peak, "traffic": None,
-                "peak_source": ("2 x " if fp8 else "") + "MEASURED_PEAKS.json bf16_tflops_sustained "
-                               "(of measured" + ("; FP8 dense rate is twice BF16's)" if fp8 else ")"),
+                "peak_source": ("2 x " if fp8 else "") + "MEASURED_PEAKS.json bf16_tflops, the "
+                               "burst figure (of measured" + ("; FP8 dense rate is twice BF16's)"
+                                                              if fp8 else ")"),
                 "algorithmic_flops_per_launch": flops, "ms_per_launch": mma_ms}
     cfg["comparisons"] = comps
     line = {
         "metric": METRIC, "value": n / (ms / 1e3), "unit": "points/s", "n_gpus": 1,
         "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u8" if wl.startswith("ubyte") else "f32",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": ("e4m3" if wl == "fbin-2m-960" else "bf16") + " tiles, f32 re-rank",
         "data": "synthetic", "config": cfg, "roofline": roof, "cpu_baseline": None,
         "clocks": clk, "e2e": None, "gpu_launches": launches,
     }
@@ -579,11 +630,15 @@ def main():
         mma_ms = statistics.median(phases["leaf_mma"]) / trees
         flops = 2.0 * DIM * st.sum_leaf_sq / trees
         achieved = flops / (mma_ms * 1e-3) / 1e12
-        peak = peaks.get("bf16_tflops_sustained", 1414.3)
+        # one launch lasts about a millisecond: the burst figure is its peak
+        peak = peaks.get("bf16_tflops", 1590.0)
         roofline = {"kernel": "k_leaf_mma (BF16 tcgen05 Gram tiles + top-k epilogue), per launch",
                     "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak, "traffic": _traffic_per_launch("k_leaf_mma"),
-                    "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)",
+                    "traffic_source": "profiles/traffic.json: DRAM bytes per launch from an ncu "
+                                      "capture of this kernel (not measured in this run)",
+                    "peak_source": ("MEASURED_PEAKS.json bf16_tflops, the burst figure (of measured)"
+                                    if "bf16_tflops" in peaks else "fallback 1590 TFLOP/s (of fallback)"),
                     "algorithmic_flops_per_launch": flops, "ms_per_launch": mma_ms,
                     "padded_tile_flops_per_launch": 2.0 * 128 * st.mma_pairs_padded / trees,
                     "note": "the epilogue (threshold filter + bitonic top-k in registers) bounds "
@@ -609,9 +664,12 @@ def main():
     line = {
         "metric": METRIC, "value": world * N_POINTS / (ms / 1e3), "unit": "points/s",
         "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 tiles, f32 re-rank" if args.mode == "mixed" else "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "mode": args.mode, "ntrees": trees,
+        "config": {"workload": WORKLOAD,
+                   "trees": TREES_MIXED if args.mode == "mixed" else TREES_REFERENCE,
+                   "mode": args.mode, "ntrees": trees,
                    "leaf_size": leaf or None, "recall@10": rec, "recall_sample": 1000,
                    "global_depth": st.global_depth, "local_depth": st.local_depth,
                    "mean_leaf": st.sum_leaf_sq / (trees * N_POINTS),

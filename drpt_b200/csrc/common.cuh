@@ -14,6 +14,10 @@ namespace drpt {
 // Last error text of the calling host thread (drpt_last_error).
 void set_error(const char *fmt, ...);
 
+// Streaming multiprocessors of the current device (grid-stride launches are
+// sized in multiples of it); 148 if the query fails.
+int device_sm_count();
+
 #define DRPT_CUDA(call)                                                                   \
   do {                                                                                    \
     cudaError_t e_ = (call);                                                              \

@@ -1165,12 +1165,7 @@ void stage_t(const LeafStageArgs &a, bool means, cudaStream_t s) {
         per_sm < 1)
       per_sm = 1;
   }
-  int sms = 148;
-  {
-    int dev = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess)
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  }
+  const int sms = device_sm_count();
   const unsigned grid =
       (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(a.n, 8 * RB), (int64_t)sms * per_sm));
   const int64_t toff = (int64_t)a.t0 * a.n;

@@ -560,7 +560,7 @@ drpt_status launch_tree_level(const TreeLevelArgs &a, int64_t max_units, cudaStr
     return DRPT_ERR_UNSUPPORTED;
   }
   // unit kernels loop over the units actually planned (grid-stride)
-  const unsigned U = (unsigned)min64(max_units, 148 * 16);
+  const unsigned U = (unsigned)min64(max_units, (int64_t)device_sm_count() * 16);
   const unsigned gn = (unsigned)ceil_div(G * 32, 256);  // warp per node
   k_plan<<<1, 1024, 0, s>>>(a);
   if (a.exact) {

@@ -129,11 +129,19 @@ extern "C" drpt_status drpt_global_trees_noalloc(const float *P, int64_t n, int3
                                                  int32_t exact, int32_t *order, int32_t *offsets,
                                                  float *medians, void *stream) {
   using namespace drpt;
-  if (!P || !order || !offsets || n < 2 || n > INT32_MAX || T <= 0 || gd <= 0 || gd > 30)
+  if (!P || !order || !offsets) {
+    set_error("drpt_global_trees_noalloc: P, order and offsets must be device pointers (got "
+              "P=%p order=%p offsets=%p)", (const void *)P, (void *)order, (void *)offsets);
     return DRPT_ERR_INVALID_ARG;
+  }
+  if (n < 2 || n > INT32_MAX || T <= 0 || gd <= 0 || gd > 30) {
+    set_error("drpt_global_trees_noalloc: n=%lld (2 .. 2^31-1), T=%d (>= 1) or gd=%d (1 .. 30) "
+              "out of range", (long long)n, T, gd);
+    return DRPT_ERR_INVALID_ARG;
+  }
   cudaStream_t s = (cudaStream_t)stream;
   if (gd == 1) {
-    const int64_t blocks = min64(ceil_div((int64_t)T * n, 256), 148 * 8);
+    const int64_t blocks = min64(ceil_div((int64_t)T * n, 256), (int64_t)device_sm_count() * 8);
     k_single_leaf<<<(unsigned)blocks, 256, 0, s>>>(n, T, order, offsets);
     DRPT_LAUNCH_CHECK();
     return DRPT_OK;

@@ -227,7 +227,11 @@ drpt_status drpt_learn_gradient(drpt_ctx *ctx, const float *Xs, int32_t S, int32
  * stored medians and returns its k <= 32 nearest points among its leaves'
  * members by exact FP32 distance, ordered by (distance, id), each point
  * once.  The index owns its memory until drpt_index_destroy; one host thread
- * at a time per index. */
+ * at a time per index.  Query calls keep their scratch in the index, so the
+ * device work of two query calls on one index must not overlap, whatever
+ * the streams they run on: wait for one call's stream before issuing the
+ * next call on another stream (a call that grows the scratch frees the old
+ * buffers). */
 typedef struct drpt_index drpt_index;
 drpt_status drpt_index_build(drpt_ctx *ctx, const drpt_build_desc *desc, const void *data,
                              int32_t *out_idx, float *out_dist, drpt_stats *stats,

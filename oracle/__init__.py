@@ -40,14 +40,19 @@ class Info(ctypes.Structure):
                 ("n_final_leaves", ctypes.c_int), ("min_global_leaf", ctypes.c_int64)]
 
 
-def build_lib() -> None:
-    """Compile libdrpt_oracle.so (and, when the reference tree exists, the
-    reference binary) with the recipe in oracle/Makefile."""
+def build_lib(reference_root: str | None = None) -> None:
+    """Compile libdrpt_oracle.so with the recipe in oracle/Makefile and, when
+    a reference checkout is named (`reference_root`, else the environment's
+    DRPT_REFERENCE_ROOT), the reference binary _ref/drpt_ref from its
+    sources.  A named root that is not a directory is an error; with none
+    named the reference binary is not built."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if os.path.isdir(os.environ.get("DRPT_REFERENCE_ROOT", "/root/reference")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref",
-                        "REF_ROOT=" + os.environ.get("DRPT_REFERENCE_ROOT", "/root/reference")],
-                       check=True)
+    root = reference_root or os.environ.get("DRPT_REFERENCE_ROOT")
+    if not root:
+        return
+    if not os.path.isdir(root):
+        raise FileNotFoundError(f"reference checkout {root!r} (DRPT_REFERENCE_ROOT) not found")
+    subprocess.run(["make", "-s", "-C", HERE, "ref", "REF_ROOT=" + root], check=True)
 
 
 def lib():
@@ -173,20 +178,32 @@ def build(X: np.ndarray, ntrees: int, nn: int, seed: int, tree_depth_ratio: floa
 
 def exact_knn(X: np.ndarray, queries: np.ndarray, k: int, chunk: int = 256):
     """FP64 brute-force k nearest neighbours of the query points (indices into
-    X), self excluded; ties ordered by index.  Returns (idx, dist)."""
+    X), self excluded; ties ordered by index.  Returns (idx, dist).
+
+    Candidates come from an FP64 norm expansion (k + 8 smallest); a row whose
+    8 extra candidates do not separate the k-th from the rest by more than
+    twice the expansion's rounding bound (ties or near-ties at the boundary)
+    is recomputed from differences over all points."""
     Xd = np.asarray(X, np.float64)
+    n = len(Xd)
     sq = np.einsum("ij,ij->i", Xd, Xd)
+    sq_max = float(sq.max()) if n else 0.0
+    extra = min(8, max(n - 1 - k, 0))
     idx_out = np.empty((len(queries), k), np.int64)
     dist_out = np.empty((len(queries), k), np.float64)
     for s in range(0, len(queries), chunk):
         q = np.asarray(queries[s:s + chunk])
         Q = Xd[q]
         d2 = sq[q][:, None] + sq[None, :] - 2.0 * (Q @ Xd.T)
-        # exact differences for the candidates near the boundary are recomputed below
         d2[np.arange(len(q)), q] = np.inf
-        part = np.argpartition(d2, k + 8, axis=1)[:, : k + 8]
+        part = np.argpartition(d2, k + extra - 1, axis=1)[:, : k + extra] if extra else \
+            np.argsort(d2, axis=1, kind="stable")[:, :k]
         for r in range(len(q)):
             cand = part[r]
+            vals = np.sort(d2[r, cand])
+            err = 1e-12 * (sq[q[r]] + sq_max + 1.0)
+            if extra and not (vals[-1] - vals[k - 1] > 2.0 * err):
+                cand = np.arange(n)  # ambiguous boundary: every point, from differences
             diff = Xd[cand] - Q[r]
             exact = np.sqrt(np.einsum("ij,ij->i", diff, diff))
             exact[cand == q[r]] = np.inf

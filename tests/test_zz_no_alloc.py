@@ -70,8 +70,12 @@ def _without_alloc(torch, P, n, T, gd, exact):
 def test_noalloc_equals_workspace_entry_on_calls_in_a_row(torch):
     # Consecutive calls of different shapes: each one starts with the previous
     # call's contents in the shared static scratch.
+    # Odd and even global depths: with even gd the last level ends in the
+    # other side of the ping-pong, and at gd = 2 the ping-pong side, the
+    # split values and the offsets side are not carved at all.
     for n, T, gd, exact in [(200_000, 4, 7, 1), (150_001, 6, 5, 0), (200_000, 4, 7, 1),
-                            (1_000, 3, 1, 1)]:
+                            (100_000, 4, 2, 1), (150_001, 6, 6, 1), (120_000, 5, 4, 0),
+                            (90_001, 3, 2, 0), (1_000, 3, 1, 1)]:
         P = _projected(torch, n, T, gd, seed=n + T + gd)
         want = _with_workspace(torch, P, n, T, gd, exact)
         got = _without_alloc(torch, P, n, T, gd, exact)
@@ -94,3 +98,30 @@ def test_noalloc_rejects_builds_beyond_its_scratch(torch):
     assert st == 1  # DRPT_ERR_INVALID_ARG
     msg = L.drpt_last_error().decode()
     assert "static scratch" in msg and "bytes" in msg
+
+
+def test_noalloc_argument_checks_set_the_error_text(torch):
+    # Every rejected argument returns DRPT_ERR_INVALID_ARG before any launch
+    # and leaves a message of its own, not the text of an earlier failure.
+    L = _lib.load()
+    P = torch.zeros((8, 64), dtype=torch.float32, device="cuda")
+    order = torch.zeros((1, 64), dtype=torch.int32, device="cuda")
+    offs = torch.zeros((1, 64), dtype=torch.int32, device="cuda")
+    s = ctypes.c_void_p(0)
+    cases = [
+        ((None, 64, 1, 3, 1, order.data_ptr(), offs.data_ptr(), None, s), "device pointers"),
+        ((P.data_ptr(), 64, 1, 3, 1, None, offs.data_ptr(), None, s), "device pointers"),
+        ((P.data_ptr(), 64, 1, 3, 1, order.data_ptr(), None, None, s), "device pointers"),
+        ((P.data_ptr(), 1, 1, 3, 1, order.data_ptr(), offs.data_ptr(), None, s), "out of range"),
+        ((P.data_ptr(), 64, 0, 3, 1, order.data_ptr(), offs.data_ptr(), None, s), "out of range"),
+        ((P.data_ptr(), 64, 1, 0, 1, order.data_ptr(), offs.data_ptr(), None, s), "out of range"),
+        ((P.data_ptr(), 64, 1, 31, 1, order.data_ptr(), offs.data_ptr(), None, s), "out of range"),
+    ]
+    for args, words in cases:
+        # plant an unrelated message first: the check must replace it
+        assert L.drpt_global_trees_noalloc(P.data_ptr(), 2_000_000, 16, 10, 1, order.data_ptr(),
+                                           offs.data_ptr(), None, s) == 1
+        assert "static scratch" in L.drpt_last_error().decode()
+        assert L.drpt_global_trees_noalloc(*args) == 1, args
+        msg = L.drpt_last_error().decode()
+        assert words in msg and "static scratch" not in msg, (args, msg)
