@@ -454,6 +454,8 @@ drpt_status mixed_leaf_phase(drpt_ctx *c, const void *X, int dtype, int64_t n, i
   DRPT_TRY(ws_get(c, "mx_err", 1, &a.err));
   DRPT_TRY(ws_get(c, "mx_run_idx", (size_t)n * kp, &a.cand_idx));
   DRPT_TRY(ws_get(c, "mx_run_dist", (size_t)n * kp, &a.cand_dist));
+  DRPT_TRY(ws_get(c, "mx_tree_idx", (size_t)n * kp, &a.tree_idx));
+  DRPT_TRY(ws_get(c, "mx_tree_dist", (size_t)n * kp, &a.tree_dist));
   DRPT_CUDA(cudaMemsetAsync(a.err, 0, sizeof(int), s));
   int nev = 0;
   if (timed) {
@@ -499,7 +501,7 @@ drpt_status mixed_leaf_phase(drpt_ctx *c, const void *X, int dtype, int64_t n, i
       a.scl = fp8 ? scl + (size_t)(t - t0) * n : scl;
       if (timed) DRPT_TRY(mark(&e0));
       DRPT_TRY(launch_leaf_mma(a, s));
-      c->launches += 2;
+      c->launches += t > 0 ? 3 : 2;  // tile plan, leaf kernel, fold
       if (timed) {
         DRPT_TRY(mark(&e1));
         c->tmma.push_back({e0, e1});

@@ -509,7 +509,8 @@ __global__ void __launch_bounds__(MmaCfg<KP, STREAM>::threads,
     const float *__restrict__ nrm, const float *__restrict__ scl,
     const int32_t *__restrict__ tile_leaf, const int32_t *__restrict__ tile_r0,
     const int32_t *__restrict__ n_tiles, int kb, int tree, int32_t *__restrict__ run_idx,
-    float *__restrict__ run_dist, int *err) {
+    float *__restrict__ run_dist, int32_t *__restrict__ tree_idx, float *__restrict__ tree_dist,
+    int *err) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
@@ -857,10 +858,12 @@ __global__ void __launch_bounds__(MmaCfg<KP, STREAM>::threads,
       }
     }
     if (grp == 0 && rvalid) {
-      // fold this tree's list into the running list: keys back to (squared
-      // distance, point id); drop neighbours the running list already holds;
-      // a bitonic merge keeps the KP best by (distance, id)
-      const int64_t o = (int64_t)my_pt * KP;
+      // this tree's list, keys back to (squared distance, point id), already
+      // ascending by key, i.e. by distance: tree 0's is the running list;
+      // later trees' go to the tree list, which k_fold_lists merges into the
+      // running list (a separate, fully parallel pass: folding here kept the
+      // CTA, its idle TMA and MMA warps and its shared memory for the
+      // latency of the running list's reads)
       float rd[KP];
       int32_t ri[KP];
 #pragma unroll
@@ -871,37 +874,13 @@ __global__ void __launch_bounds__(MmaCfg<KP, STREAM>::threads,
         rd[j] = have ? nr + __uint_as_float(key & ~kColMask) : __int_as_float(0x7f800000);
         ri[j] = q;
       }
-      if (tree > 0) {
-        float od[KP];
-        int32_t oi[KP];
+      const int64_t o = (int64_t)my_pt * KP;
+      float4 *dd = reinterpret_cast<float4 *>((tree > 0 ? tree_dist : run_dist) + o);
+      int4 *di = reinterpret_cast<int4 *>((tree > 0 ? tree_idx : run_idx) + o);
 #pragma unroll
-        for (int j = 0; j < KP; ++j) {
-          od[j] = run_dist[o + j];
-          oi[j] = run_idx[o + j];
-        }
-#pragma unroll
-        for (int j = 0; j < KP; ++j) {
-          bool dup = false;
-#pragma unroll
-          for (int i = 0; i < KP; ++i) dup |= (ri[j] >= 0 && oi[i] == ri[j]);
-          if (dup) {
-            ri[j] = -1;
-            rd[j] = __int_as_float(0x7f800000);
-          }
-        }
-        bitonic_sort<KP>(rd, ri);
-        bitonic_merge_into<KP, KP>(od, oi, rd, ri);
-#pragma unroll
-        for (int j = 0; j < KP; ++j) {
-          rd[j] = od[j];
-          ri[j] = oi[j];
-        }
-      }
-      // (tree 0: the list is already ascending by key, i.e. by distance)
-#pragma unroll
-      for (int j = 0; j < KP; ++j) {
-        run_dist[o + j] = rd[j];
-        run_idx[o + j] = ri[j];
+      for (int j = 0; j < KP; j += 4) {
+        dd[j / 4] = make_float4(rd[j], rd[j + 1], rd[j + 2], rd[j + 3]);
+        di[j / 4] = make_int4(ri[j], ri[j + 1], ri[j + 2], ri[j + 3]);
       }
     }
   }
@@ -912,6 +891,51 @@ __global__ void __launch_bounds__(MmaCfg<KP, STREAM>::threads,
     tmem_dealloc(tmem, 128);
   }
   if (threadIdx.x == 0 && *abort_flag) atomicOr(err, 1);
+}
+
+// k_fold_lists: per point (one thread each), fold this tree's list (KP
+// candidates ascending by approximate distance) into the running list of the
+// KP best distinct candidates of the trees before: neighbours the running
+// list already holds are dropped from the new list, which is re-sorted, and a
+// bitonic merge keeps the KP best by distance.
+template <int KP>
+__global__ void __launch_bounds__(256) k_fold_lists(const float *__restrict__ tree_dist,
+                                                    const int32_t *__restrict__ tree_idx,
+                                                    int64_t n, float *__restrict__ run_dist,
+                                                    int32_t *__restrict__ run_idx) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int64_t o = p * KP;
+  float rd[KP], od[KP];
+  int32_t ri[KP], oi[KP];
+#pragma unroll
+  for (int j = 0; j < KP; j += 4) {
+    const float4 a = __ldcs(reinterpret_cast<const float4 *>(tree_dist + o) + j / 4);
+    const int4 b = __ldcs(reinterpret_cast<const int4 *>(tree_idx + o) + j / 4);
+    const float4 c = reinterpret_cast<const float4 *>(run_dist + o)[j / 4];
+    const int4 e = reinterpret_cast<const int4 *>(run_idx + o)[j / 4];
+    rd[j] = a.x; rd[j + 1] = a.y; rd[j + 2] = a.z; rd[j + 3] = a.w;
+    ri[j] = b.x; ri[j + 1] = b.y; ri[j + 2] = b.z; ri[j + 3] = b.w;
+    od[j] = c.x; od[j + 1] = c.y; od[j + 2] = c.z; od[j + 3] = c.w;
+    oi[j] = e.x; oi[j + 1] = e.y; oi[j + 2] = e.z; oi[j + 3] = e.w;
+  }
+#pragma unroll
+  for (int j = 0; j < KP; ++j) {
+    bool dup = false;
+#pragma unroll
+    for (int i = 0; i < KP; ++i) dup |= (ri[j] >= 0 && oi[i] == ri[j]);
+    if (dup) {
+      ri[j] = -1;
+      rd[j] = __int_as_float(0x7f800000);
+    }
+  }
+  bitonic_sort<KP>(rd, ri);
+  bitonic_merge_into<KP, KP>(od, oi, rd, ri);
+#pragma unroll
+  for (int j = 0; j < KP; j += 4) {
+    reinterpret_cast<float4 *>(run_dist + o)[j / 4] = make_float4(od[j], od[j + 1], od[j + 2], od[j + 3]);
+    reinterpret_cast<int4 *>(run_idx + o)[j / 4] = make_int4(oi[j], oi[j + 1], oi[j + 2], oi[j + 3]);
+  }
 }
 
 // ------------------------------------------------------------------ K11
@@ -1198,8 +1222,13 @@ drpt_status mma_t(const MixedTreeArgs &a, const CUtensorMap &tmA, int kb, cudaSt
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_leaf_mma<KP, STREAM, FP8><<<grid, Cfg::threads, smem, s>>>(
       tmA, tmB, a.goff, a.order, a.nrm, a.scl, a.tile_leaf, a.tile_r0, a.n_tiles, kb, a.tree,
-      a.cand_idx, a.cand_dist, a.err);
+      a.cand_idx, a.cand_dist, a.tree_idx, a.tree_dist, a.err);
   DRPT_LAUNCH_CHECK();
+  if (a.tree > 0) {
+    k_fold_lists<KP><<<(unsigned)ceil_div(a.n, 256), 256, 0, s>>>(a.tree_dist, a.tree_idx, a.n,
+                                                                  a.cand_dist, a.cand_idx);
+    DRPT_LAUNCH_CHECK();
+  }
   return DRPT_OK;
 }
 

@@ -109,6 +109,8 @@ struct MixedTreeArgs {
   int32_t *tile_leaf, *tile_r0, *n_tiles;  // n / 128 + nleaf
   int32_t *cand_idx;         // n x kp running list (point ids), updated tree by tree
   float *cand_dist;          // n x kp approximate squared distances, ascending
+  int32_t *tree_idx;         // n x kp: this tree's list (trees after the first),
+  float *tree_dist;          // folded into the running list after the leaf kernel
   int *err;                  // set when a bounded wait gave up
 };
 int mixed_d_pad(int d, int fp8);
