@@ -28,7 +28,7 @@ EXPORTS = [
     "drpt_host_projection", "drpt_project", "drpt_global_trees", "drpt_local_leaves",
     "drpt_leaf_knn", "drpt_merge_candidates", "drpt_global_trees_noalloc",
     "drpt_build_graph_batched", "drpt_learn_gradient", "drpt_index_build", "drpt_index_query",
-    "drpt_index_destroy", "drpt_locality_slots",
+    "drpt_index_destroy", "drpt_locality_slots", "drpt_build_graph_stream",
 ]
 
 
@@ -110,6 +110,9 @@ def load(path: str = LIB_PATH):
         L.drpt_ctx_destroy.restype = None
         L.drpt_build_graph.argtypes = [vp, ctypes.POINTER(BuildDesc), vp, vp, vp,
                                        ctypes.POINTER(Stats)]
+        L.drpt_build_graph_stream.argtypes = [vp, ctypes.POINTER(BuildDesc), i32,
+                                              ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                              ctypes.POINTER(vp), ctypes.POINTER(Stats)]
         L.drpt_host_projection.argtypes = [u32, i32, i32, ctypes.c_float, vp]
         L.drpt_project.argtypes = [vp, vp, i64, i32, i32, vp, i32, vp, i32, vp, vp]
         L.drpt_global_trees.argtypes = [vp, vp, i64, i32, i32, i32, vp, vp, vp, vp]

@@ -840,8 +840,12 @@ drpt_status dev_copy(Tp **dst, const void *src, size_t count, cudaStream_t s) {
   return DRPT_OK;
 }
 
+// check = false leaves the leaf kernel's error flag for the caller to read
+// (no host synchronisation; with stats == nullptr and keep == nullptr the
+// build of random trees is then fully stream-ordered).
 drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, int32_t *oi,
-                      float *od, drpt_stats *stats, cudaStream_t s, drpt_index *keep = nullptr) {
+                      float *od, drpt_stats *stats, cudaStream_t s, drpt_index *keep = nullptr,
+                      bool check = true) {
   const int64_t n = desc->n;
   const int d = desc->d, T = desc->ntrees, nn = desc->nn;
   if (nn > 32) {
@@ -911,7 +915,7 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
 
   DRPT_TRY(mixed_leaf_phase(c, X, desc->dtype, n, d, T, nn, kp, fp8, order, goff, nleaf, oi, od,
                             /*timed=*/true, s));
-  DRPT_TRY(mixed_check(c, s));
+  if (check) DRPT_TRY(mixed_check(c, s));
   if (keep) {
     // the index keeps its own copies: the workspace is reused by later calls
     keep->n = n;
@@ -1714,6 +1718,139 @@ static drpt_status build_graph_impl(drpt_ctx *c, const drpt_build_desc *desc, co
 drpt_status drpt_build_graph(drpt_ctx *c, const drpt_build_desc *desc, const void *data,
                              int32_t *out_idx, float *out_dist, drpt_stats *stats) {
   return build_graph_impl(c, desc, data, out_idx, out_dist, stats, nullptr);
+}
+
+// Many same-shape builds from host memory, pipelined: job j's rows go to
+// device buffer j % 2 on an input-copy stream, its build runs on the compute
+// stream once they have landed (and once job j - 2's lists have left output
+// buffer j % 2), and its lists go back on an output-copy stream.  So the
+// input copy of job j + 1 and the output copy of job j - 1 overlap the build
+// of job j.  The leaf kernel's error flag of every job is kept on the device
+// and read once at the end.
+drpt_status drpt_build_graph_stream(drpt_ctx *c, const drpt_build_desc *desc, int32_t count,
+                                    const void *const *data, int32_t *const *out_idx,
+                                    float *const *out_dist, drpt_stats *stats) {
+  if (!c || !desc || !data || !out_idx || count < 1) {
+    set_error("drpt_build_graph_stream: null argument or count < 1");
+    return DRPT_ERR_INVALID_ARG;
+  }
+  if (desc->mode != DRPT_MODE_MIXED || desc->data_on_device || desc->out_on_device) {
+    set_error("drpt_build_graph_stream: mixed mode with host inputs and outputs only");
+    return DRPT_ERR_INVALID_ARG;
+  }
+  for (int32_t j = 0; j < count; ++j)
+    if (!data[j] || !out_idx[j]) {
+      set_error("drpt_build_graph_stream: job %d has a null input or output", j);
+      return DRPT_ERR_INVALID_ARG;
+    }
+  DRPT_TRY(check_common(desc));
+  DRPT_CUDA(cudaSetDevice(c->device));
+  const int64_t n = desc->n;
+  const int nn = desc->nn;
+  const size_t in_bytes = (size_t)n * desc->d * (desc->dtype == DRPT_DTYPE_U8 ? 1 : 4);
+  const size_t out_bytes = (size_t)n * nn * 4;
+  uint8_t *xb[2];
+  int32_t *ob_i[2];
+  float *ob_d[2];
+  int *errs = nullptr;
+  DRPT_TRY(ws_get(c, "st_x0", in_bytes, &xb[0]));
+  DRPT_TRY(ws_get(c, "st_x1", in_bytes, &xb[1]));
+  DRPT_TRY(ws_get(c, "st_oi0", (size_t)n * nn, &ob_i[0]));
+  DRPT_TRY(ws_get(c, "st_oi1", (size_t)n * nn, &ob_i[1]));
+  DRPT_TRY(ws_get(c, "st_od0", (size_t)n * nn, &ob_d[0]));
+  DRPT_TRY(ws_get(c, "st_od1", (size_t)n * nn, &ob_d[1]));
+  DRPT_TRY(ws_get(c, "st_errs", (size_t)count, &errs));
+  // streams and events of this call
+  cudaStream_t comp = (cudaStream_t)desc->stream, sin = nullptr, sout = nullptr;
+  cudaEvent_t ev_in[2] = {}, ev_comp[2] = {}, ev_out[2] = {}, t0 = nullptr, t1 = nullptr;
+  drpt_status st = DRPT_OK;
+  auto cu = [&](cudaError_t e, const char *what) {
+    if (e != cudaSuccess && st == DRPT_OK) {
+      set_error("%s: %s", what, cudaGetErrorString(e));
+      st = DRPT_ERR_CUDA;
+    }
+    return st == DRPT_OK;
+  };
+  cu(cudaStreamCreateWithFlags(&sin, cudaStreamNonBlocking), "cudaStreamCreate");
+  cu(cudaStreamCreateWithFlags(&sout, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (int b = 0; b < 2; ++b) {
+    cu(cudaEventCreateWithFlags(&ev_in[b], cudaEventDisableTiming), "cudaEventCreate");
+    cu(cudaEventCreateWithFlags(&ev_comp[b], cudaEventDisableTiming), "cudaEventCreate");
+    cu(cudaEventCreateWithFlags(&ev_out[b], cudaEventDisableTiming), "cudaEventCreate");
+  }
+  cu(cudaEventCreate(&t0), "cudaEventCreate");
+  cu(cudaEventCreate(&t1), "cudaEventCreate");
+  const int launches0 = c->launches;
+  drpt_build_desc d = *desc;
+  d.data_on_device = 1;
+  d.out_on_device = 1;
+  d.stream = comp;
+  if (st == DRPT_OK) cu(cudaEventRecord(t0, sin), "cudaEventRecord");
+  for (int32_t j = 0; st == DRPT_OK && j < count; ++j) {
+    const int b = j & 1;
+    // job j - 2's build is done with input buffer b
+    if (j >= 2 && !cu(cudaStreamWaitEvent(sin, ev_comp[b], 0), "cudaStreamWaitEvent")) break;
+    if (!cu(cudaMemcpyAsync(xb[b], data[j], in_bytes, cudaMemcpyHostToDevice, sin),
+            "cudaMemcpyAsync")) break;
+    cu(cudaEventRecord(ev_in[b], sin), "cudaEventRecord");
+    cu(cudaStreamWaitEvent(comp, ev_in[b], 0), "cudaStreamWaitEvent");
+    // job j - 2's lists have left output buffer b
+    if (j >= 2) cu(cudaStreamWaitEvent(comp, ev_out[b], 0), "cudaStreamWaitEvent");
+    if (st != DRPT_OK) break;
+    st = run_mixed(c, &d, xb[b], ob_i[b], ob_d[b], nullptr, comp, nullptr, /*check=*/false);
+    if (st != DRPT_OK) break;
+    int *err_d = nullptr;
+    st = ws_get(c, "mx_err", 1, &err_d);
+    if (st != DRPT_OK) break;
+    cu(cudaMemcpyAsync(errs + j, err_d, sizeof(int), cudaMemcpyDeviceToDevice, comp),
+       "cudaMemcpyAsync");
+    cu(cudaEventRecord(ev_comp[b], comp), "cudaEventRecord");
+    cu(cudaStreamWaitEvent(sout, ev_comp[b], 0), "cudaStreamWaitEvent");
+    cu(cudaMemcpyAsync(out_idx[j], ob_i[b], out_bytes, cudaMemcpyDeviceToHost, sout),
+       "cudaMemcpyAsync");
+    if (out_dist && out_dist[j])
+      cu(cudaMemcpyAsync(out_dist[j], ob_d[b], out_bytes, cudaMemcpyDeviceToHost, sout),
+         "cudaMemcpyAsync");
+    cu(cudaEventRecord(ev_out[b], sout), "cudaEventRecord");
+  }
+  // everything issued so far is waited for, also after a failure
+  if (sin) cudaStreamSynchronize(sin);
+  cudaStreamSynchronize(comp);
+  if (sout) {
+    if (st == DRPT_OK) cu(cudaEventRecord(t1, sout), "cudaEventRecord");
+    cudaStreamSynchronize(sout);
+  }
+  if (st == DRPT_OK) {
+    std::vector<int> he((size_t)count);
+    if (cu(cudaMemcpy(he.data(), errs, (size_t)count * sizeof(int), cudaMemcpyDeviceToHost),
+           "cudaMemcpy")) {
+      int any = 0;
+      for (int e : he) any |= e;
+      if (any & 2) {
+        set_error("a global leaf holds more than 8192 points (the tensor-core leaf kernel's "
+                  "limit); use a smaller leaf_size");
+        st = DRPT_ERR_UNSUPPORTED;
+      } else if (any) {
+        set_error("a bounded wait in the tensor-core leaf kernel gave up");
+        st = DRPT_ERR_TIMEOUT;
+      }
+    }
+  }
+  if (st == DRPT_OK && stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->kernels_launched = c->launches - launches0;
+    cu(cudaEventElapsedTime(&stats->ms_total, t0, t1), "cudaEventElapsedTime");
+  }
+  for (int b = 0; b < 2; ++b) {
+    if (ev_in[b]) cudaEventDestroy(ev_in[b]);
+    if (ev_comp[b]) cudaEventDestroy(ev_comp[b]);
+    if (ev_out[b]) cudaEventDestroy(ev_out[b]);
+  }
+  if (t0) cudaEventDestroy(t0);
+  if (t1) cudaEventDestroy(t1);
+  if (sin) cudaStreamDestroy(sin);
+  if (sout) cudaStreamDestroy(sout);
+  return st;
 }
 
 static void index_free(drpt_index *x) {

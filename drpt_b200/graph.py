@@ -20,8 +20,8 @@ import numpy as np
 from . import _lib
 from ._lib import DrptError, Stats, check
 
-__all__ = ["build_graph", "build_graph_batched", "build_index", "Index", "MDRPT", "DrptError",
-           "edge_list_lines", "global_depth"]
+__all__ = ["build_graph", "build_graph_batched", "build_graph_stream", "build_index", "Index",
+           "MDRPT", "DrptError", "edge_list_lines", "global_depth"]
 
 
 def _torch():
@@ -134,6 +134,48 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
         check(_lib.load().drpt_build_graph(ctx.handle, ctypes.byref(desc), ptr_data, ptr_idx,
                                            ptr_dist, ctypes.byref(stats)))
     return idx, dist, stats
+
+
+def build_graph_stream(datasets, ntrees: int, nn: int, seed: int, *, leaf_size: int = 0,
+                       precision: str = "bf16", list_width: int = 0, density: float = 0.0,
+                       outs=None, stream=None, device: int = 0):
+    """Mixed-form graphs of many same-shape host datasets, pipelined
+    (drpt_build_graph_stream): dataset j's copy to the device and the copy of
+    dataset j - 1's lists back run on their own streams while graph j is
+    built.  `datasets`: NumPy arrays of one shape and dtype (pinned memory
+    lets the copies overlap); `outs`: optional list of (idx, dist) host arrays.
+    Returns (list of (idx, dist), stats); each graph equals build_graph's of
+    the same dataset."""
+    datasets = [np.ascontiguousarray(x) for x in datasets]
+    if not datasets:
+        raise ValueError("no datasets")
+    n, d = int(datasets[0].shape[0]), int(datasets[0].shape[1])
+    code = _dtype_code(datasets[0])
+    for x in datasets:
+        if x.shape != datasets[0].shape or _dtype_code(x) != code:
+            raise ValueError("every dataset must have the same shape and dtype")
+    if outs is None:
+        outs = [(np.empty((n, nn), np.int32), np.empty((n, nn), np.float32)) for _ in datasets]
+    desc = _lib.BuildDesc()
+    desc.n, desc.d, desc.dtype = n, d, code
+    desc.ntrees, desc.nn = ntrees, nn
+    desc.tree_depth_ratio, desc.local_tree_offset, desc.tree_depth = 0.6, 2, 0
+    desc.density, desc.seed = density, seed & 0xFFFFFFFF
+    desc.mode = _lib.MODE_MIXED
+    desc.leaf_size = leaf_size
+    desc.precision = {"bf16": _lib.PRECISION_BF16, "fp8": _lib.PRECISION_FP8_E4M3}[precision]
+    desc.list_width = list_width
+    desc.data_on_device = desc.out_on_device = 0
+    desc.stream = stream or 0
+    k = len(datasets)
+    data_p = (ctypes.c_void_p * k)(*[x.ctypes.data for x in datasets])
+    idx_p = (ctypes.c_void_p * k)(*[o[0].ctypes.data for o in outs])
+    dist_p = (ctypes.c_void_p * k)(*[o[1].ctypes.data for o in outs])
+    stats = Stats()
+    ctx = _lib.context(device)
+    check(_lib.load().drpt_build_graph_stream(ctx.handle, ctypes.byref(desc), k, data_p, idx_p,
+                                              dist_p, ctypes.byref(stats)))
+    return outs, stats
 
 
 class Index:

@@ -168,6 +168,22 @@ void drpt_ctx_destroy(drpt_ctx *ctx);
 drpt_status drpt_build_graph(drpt_ctx *ctx, const drpt_build_desc *desc, const void *data,
                              int32_t *out_idx, float *out_dist, drpt_stats *stats);
 
+/* Many k-NN-graph builds of the same shape from host memory, pipelined (no
+ * reference counterpart: the reference reads one dataset, builds and writes
+ * its edge list per run, main.cpp:156-233).  desc->mode must be
+ * DRPT_MODE_MIXED with host inputs and outputs (data_on_device and
+ * out_on_device 0); desc->stream (NULL = legacy default) carries the device
+ * work.  Job j reads data[j] (n x d rows) and writes out_idx[j] and, when
+ * out_dist and out_dist[j] are not NULL, out_dist[j] (n x nn each), as
+ * drpt_build_graph would.  The input copy of job j + 1 and the output copy of
+ * job j - 1 run on their own streams while job j builds; pinned host memory
+ * lets them overlap.  Returns when every job has finished; stats (may be
+ * NULL) gets the kernels launched and, in ms_total, the device time from the
+ * first input copy to the last output copy. */
+drpt_status drpt_build_graph_stream(drpt_ctx *ctx, const drpt_build_desc *desc, int32_t count,
+                                    const void *const *data, int32_t *const *out_idx,
+                                    float *const *out_dist, drpt_stats *stats);
+
 /* A batch of independent k-NN-graph builds (no reference counterpart: the
  * reference builds one dataset per process run).  The datasets share d,
  * dtype and the build parameters and lie row-wise one after another in
