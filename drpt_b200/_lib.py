@@ -19,7 +19,7 @@ STATUS_NAMES = {
     6: "DRPT_ERR_CUDA", 7: "DRPT_ERR_TIMEOUT", 8: "DRPT_ERR_UNSUPPORTED",
 }
 DTYPE_F32, DTYPE_U8 = 0, 1
-MODE_EXACT, MODE_FAST, MODE_MIXED, MODE_FP32_LEAF = 0, 1, 2, 3
+MODE_EXACT, MODE_FAST, MODE_MIXED, MODE_FP32_LEAF, MODE_FP32_GRAM = 0, 1, 2, 3, 4
 PRECISION_BF16, PRECISION_FP8_E4M3 = 0, 1
 
 # Every symbol include/drpt_gpu.h declares.

@@ -19,9 +19,19 @@ LIB = os.path.join(PKG, "libdrpt_gpu.so")
 CLI = os.path.join(PKG, "drpt")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
+NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                   "-Xcompiler", "-O2", "-Xptxas", "-O3", "--expt-relaxed-constexpr",
                   "-I" + INCLUDE, "-I" + CSRC]
+# The reference-exact kernels reproduce the reference's FP32 operation
+# sequences (projection sums, node statistics, medians, per-pair distances),
+# so nothing in them may be contracted into a fused multiply-add; the other
+# kernels (mixed form, FP32 Gram form, queries, learned splits) may.
+EXACT_SOURCES = {"api.cu", "k_project.cu", "k_tree.cu", "k_local.cu", "k_leafknn.cu",
+                 "k_merge.cu", "noalloc.cu", "host_algo.cpp"}
+
+
+def _fmad_flag(src: str) -> str:
+    return "-fmad=false" if os.path.basename(src) in EXACT_SOURCES else "-fmad=true"
 
 
 def _nvcc() -> str:
@@ -57,7 +67,7 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
     objs = []
     for src in lib_sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
-        cmd = [_nvcc(), "-ccbin", _host_cxx()] + NVFLAGS + ["-c", src, "-o", obj]
+        cmd = [_nvcc(), "-ccbin", _host_cxx()] + NVFLAGS + [_fmad_flag(src), "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -364,7 +364,7 @@ drpt_status check_common(const drpt_build_desc *d) {
   if (!d) return DRPT_ERR_INVALID_ARG;
   if (d->n < 2 || d->n > INT32_MAX || d->d <= 0 || d->ntrees <= 0 || d->nn <= 0 ||
       (d->dtype != DRPT_DTYPE_F32 && d->dtype != DRPT_DTYPE_U8) || !(d->tree_depth_ratio > 0) ||
-      (d->mode < DRPT_MODE_EXACT || d->mode > DRPT_MODE_FP32_LEAF)) {
+      (d->mode < DRPT_MODE_EXACT || d->mode > DRPT_MODE_FP32_GRAM)) {
     set_error("invalid descriptor (n=%lld d=%d ntrees=%d nn=%d dtype=%d mode=%d)",
               (long long)d->n, d->d, d->ntrees, d->nn, d->dtype, d->mode);
     return DRPT_ERR_INVALID_ARG;
@@ -408,9 +408,12 @@ int list_width_of(int req, int nn) {
   return (req == 16 || req == 32) && req >= nn ? req : -1;
 }
 
+// f32gram: the leaf Gram tiles in FP32 on the CUDA cores over the rows of X
+// (no staging) instead of BF16 / E4M3 tiles on the tensor cores.
 drpt_status mixed_leaf_phase(drpt_ctx *c, const void *X, int dtype, int64_t n, int d, int T,
                              int nn, int kp, int fp8, const int32_t *order, const int32_t *goff,
-                             int nleaf, int32_t *oi, float *od, bool timed, cudaStream_t s) {
+                             int nleaf, int32_t *oi, float *od, bool timed, cudaStream_t s,
+                             bool f32gram = false) {
   const int d_pad = mixed_d_pad(d, fp8);
   cudaEvent_t *ev = c->ev;
   MixedTreeArgs a{};
@@ -423,13 +426,17 @@ drpt_status mixed_leaf_phase(drpt_ctx *c, const void *X, int dtype, int64_t n, i
   a.T = T;
   a.kp = kp;
   a.fp8 = fp8;
-  const int Tc = mixed_stage_trees(n, d_pad, fp8, T);
+  const int Tc = f32gram ? T : mixed_stage_trees(n, d_pad, fp8, T);
   const size_t row_bytes = (size_t)d_pad * (fp8 ? 1 : 2);
   uint8_t *xb = nullptr;
   float *nrm = nullptr, *scl = nullptr;
-  DRPT_TRY(ws_get(c, "mx_xb", (size_t)Tc * n * row_bytes, &xb));
-  DRPT_TRY(ws_get(c, "mx_nrm", (size_t)Tc * n, &nrm));
-  DRPT_TRY(ws_get(c, "mx_scl", fp8 ? (size_t)Tc * n : 1, &scl));
+  if (!f32gram) {
+    DRPT_TRY(ws_get(c, "mx_xb", (size_t)Tc * n * row_bytes, &xb));
+    DRPT_TRY(ws_get(c, "mx_nrm", (size_t)Tc * n, &nrm));
+    DRPT_TRY(ws_get(c, "mx_scl", fp8 ? (size_t)Tc * n : 1, &scl));
+  } else {
+    DRPT_TRY(ws_get(c, "fg_nrm", (size_t)n, &nrm));  // ||x||^2, the same for every tree
+  }
   LeafStageArgs st{};
   st.X = X;
   st.dtype = dtype;
@@ -441,13 +448,15 @@ drpt_status mixed_leaf_phase(drpt_ctx *c, const void *X, int dtype, int64_t n, i
   st.goff = goff;
   st.nleaf = nleaf;
   st.T = T;
-  DRPT_TRY(ws_get(c, "mx_pos", (size_t)T * n, &st.pos));
-  DRPT_TRY(ws_get(c, "mx_lf", (size_t)T * n, &st.lf));
-  DRPT_TRY(ws_get(c, "mx_mu", (size_t)T * nleaf * d, &st.mu));
+  if (!f32gram) {
+    DRPT_TRY(ws_get(c, "mx_pos", (size_t)T * n, &st.pos));
+    DRPT_TRY(ws_get(c, "mx_lf", (size_t)T * n, &st.lf));
+    DRPT_TRY(ws_get(c, "mx_mu", (size_t)T * nleaf * d, &st.mu));
+  }
   st.Xb = xb;
   st.nrm = nrm;
   st.scl = scl;
-  const size_t tiles = (size_t)ceil_div(n, 128) + nleaf;
+  const size_t tiles = (size_t)ceil_div(n, 64) + nleaf;  // the FP32 form's 64-row tiles
   DRPT_TRY(ws_get(c, "mx_tile_leaf", tiles, &a.tile_leaf));
   DRPT_TRY(ws_get(c, "mx_tile_r0", tiles, &a.tile_r0));
   DRPT_TRY(ws_get(c, "mx_n_tiles", 1, &a.n_tiles));
@@ -475,6 +484,34 @@ drpt_status mixed_leaf_phase(drpt_ctx *c, const void *X, int dtype, int64_t n, i
     return DRPT_OK;
   };
   int e0 = 0, e1 = 0;
+  if (f32gram) {
+    if (timed) DRPT_TRY(mark(&e0));
+    DRPT_TRY(launch_row_norms(X, dtype, n, d, nrm, s));
+    c->launches += 1;
+    if (timed) {
+      DRPT_TRY(mark(&e1));
+      c->tstage.push_back({e0, e1});
+    }
+    a.nrm = nrm;
+    for (int t = 0; t < T; ++t) {
+      a.tree = t;
+      a.order = order + (size_t)t * n;
+      a.goff = goff + (size_t)t * (nleaf + 1);
+      if (timed) DRPT_TRY(mark(&e0));
+      DRPT_TRY(launch_leaf_f32(a, nrm, s));
+      c->launches += t > 0 ? 3 : 2;  // tile plan, leaf kernel, fold
+      if (timed) {
+        DRPT_TRY(mark(&e1));
+        c->tmma.push_back({e0, e1});
+      }
+    }
+    if (timed) DRPT_CUDA(cudaEventRecord(ev[4], s));
+    DRPT_TRY(launch_rerank(X, dtype, d, order + (size_t)(T - 1) * n, n, a.cand_idx, kp, nn, oi,
+                           od, s));
+    c->launches += 1;
+    if (timed) DRPT_CUDA(cudaEventRecord(ev[5], s));
+    return DRPT_OK;
+  }
   if (timed) DRPT_TRY(mark(&e0));
   DRPT_TRY(launch_leaf_means(st, s));
   c->launches += 2;
@@ -861,9 +898,14 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
     set_error("unknown precision %d", desc->precision);
     return DRPT_ERR_INVALID_ARG;
   }
-  const int fp8 = desc->precision == DRPT_PRECISION_FP8_E4M3;
+  const bool f32gram = desc->mode == DRPT_MODE_FP32_GRAM;
+  const int fp8 = !f32gram && desc->precision == DRPT_PRECISION_FP8_E4M3;
   if (d % 4 != 0 || d > 1024) {
     set_error("mixed mode supports d %% 4 == 0 and d <= 1024 (got %d)", d);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  if (f32gram && (d % 8 != 0 || desc->learned_trees != 0)) {
+    set_error("the FP32 Gram form needs d %% 8 == 0 and no learned trees (d = %d)", d);
     return DRPT_ERR_UNSUPPORTED;
   }
   const int learned = desc->learned_trees;
@@ -914,7 +956,7 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
   DRPT_CUDA(cudaEventRecord(ev[2], s));
 
   DRPT_TRY(mixed_leaf_phase(c, X, desc->dtype, n, d, T, nn, kp, fp8, order, goff, nleaf, oi, od,
-                            /*timed=*/true, s));
+                            /*timed=*/true, s, f32gram));
   if (check) DRPT_TRY(mixed_check(c, s));
   if (keep) {
     // the index keeps its own copies: the workspace is reused by later calls
@@ -1598,7 +1640,8 @@ static drpt_status build_graph_impl(drpt_ctx *c, const drpt_build_desc *desc, co
     X = xd;
   }
 
-  if (desc->mode == DRPT_MODE_MIXED || desc->mode == DRPT_MODE_FP32_LEAF) {
+  if (desc->mode == DRPT_MODE_MIXED || desc->mode == DRPT_MODE_FP32_LEAF ||
+      desc->mode == DRPT_MODE_FP32_GRAM) {
     int32_t *oi = out_idx;
     float *od = out_dist;
     if (!desc->out_on_device) {
@@ -1607,7 +1650,8 @@ static drpt_status build_graph_impl(drpt_ctx *c, const drpt_build_desc *desc, co
     } else if (!od) {
       DRPT_TRY(ws_get(c, "out_dist", (size_t)n * nn, &od));
     }
-    if (desc->mode == DRPT_MODE_MIXED) DRPT_TRY(run_mixed(c, desc, X, oi, od, stats, s, keep));
+    if (desc->mode == DRPT_MODE_MIXED || desc->mode == DRPT_MODE_FP32_GRAM)
+      DRPT_TRY(run_mixed(c, desc, X, oi, od, stats, s, keep));
     else DRPT_TRY(run_fp32_leaf(c, desc, X, oi, od, stats, s));
     if (!desc->out_on_device) {
       DRPT_CUDA(cudaMemcpyAsync(out_idx, oi, (size_t)n * nn * 4, cudaMemcpyDeviceToHost, s));

@@ -11,7 +11,7 @@
 //
 // Flags added here: -seed (projection seed; default drawn from
 // std::random_device as the reference draws it, mdrpt.cpp:402-416, and
-// printed), -mode exact|fast|mixed|fp32_leaf (default exact), -leaf-size,
+// printed), -mode exact|fast|mixed|fp32_leaf|fp32_gram (default exact), -leaf-size,
 // -tree-depth, -device.  -locality 1 runs the reference's locality
 // relabelling in the exact and fast modes (off unless given: at one rank it
 // only renumbers global leaves and the graph is the same).
@@ -73,7 +73,8 @@ int parse_mode(const char *s) {
   if (!std::strcmp(s, "fast")) return DRPT_MODE_FAST;
   if (!std::strcmp(s, "mixed")) return DRPT_MODE_MIXED;
   if (!std::strcmp(s, "fp32_leaf")) return DRPT_MODE_FP32_LEAF;
-  die("-mode must be exact, fast, mixed or fp32_leaf");
+  if (!std::strcmp(s, "fp32_gram")) return DRPT_MODE_FP32_GRAM;
+  die("-mode must be exact, fast, mixed, fp32_leaf or fp32_gram");
 }
 
 Options parse(int argc, char **argv) {

@@ -334,15 +334,16 @@ __global__ void __launch_bounds__(256, StageCfg<NCH>::min_blocks) k_leaf_stage(c
 }
 
 // ------------------------------------------------------------------ K9
+// Row tiles of `rows` rows of every leaf, in leaf order.
 __global__ void __launch_bounds__(1024) k_tile_plan(const int32_t *__restrict__ goff, int nleaf,
-                                                    int32_t *tile_leaf, int32_t *tile_r0,
-                                                    int32_t *n_tiles) {
+                                                    int rows, int32_t *tile_leaf,
+                                                    int32_t *tile_r0, int32_t *n_tiles) {
   __shared__ int warp_tot[32];
   const int per = (nleaf + 1023) / 1024;
   const int j0 = threadIdx.x * per;
   int cnt = 0;
   for (int i = 0; i < per; ++i)
-    if (j0 + i < nleaf) cnt += (goff[j0 + i + 1] - goff[j0 + i] + kTM - 1) / kTM;
+    if (j0 + i < nleaf) cnt += (goff[j0 + i + 1] - goff[j0 + i] + rows - 1) / rows;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int x = cnt;
 #pragma unroll
@@ -366,10 +367,10 @@ __global__ void __launch_bounds__(1024) k_tile_plan(const int32_t *__restrict__ 
   for (int i = 0; i < per; ++i) {
     const int j = j0 + i;
     if (j >= nleaf) break;
-    const int nt = (goff[j + 1] - goff[j] + kTM - 1) / kTM;
+    const int nt = (goff[j + 1] - goff[j] + rows - 1) / rows;
     for (int q = 0; q < nt; ++q) {
       tile_leaf[base + q] = j;
-      tile_r0[base + q] = q * kTM;
+      tile_r0[base + q] = q * rows;
     }
     base += nt;
   }
@@ -1224,11 +1225,7 @@ drpt_status mma_t(const MixedTreeArgs &a, const CUtensorMap &tmA, int kb, cudaSt
       tmA, tmB, a.goff, a.order, a.nrm, a.scl, a.tile_leaf, a.tile_r0, a.n_tiles, kb, a.tree,
       a.cand_idx, a.cand_dist, a.tree_idx, a.tree_dist, a.err);
   DRPT_LAUNCH_CHECK();
-  if (a.tree > 0) {
-    k_fold_lists<KP><<<(unsigned)ceil_div(a.n, 256), 256, 0, s>>>(a.tree_dist, a.tree_idx, a.n,
-                                                                  a.cand_dist, a.cand_idx);
-    DRPT_LAUNCH_CHECK();
-  }
+  if (a.tree > 0) DRPT_TRY(launch_fold_lists(a, s));
   return DRPT_OK;
 }
 
@@ -1285,7 +1282,7 @@ drpt_status launch_leaf_mma(const MixedTreeArgs &a, cudaStream_t s) {
     set_error("mixed leaf kernel: padded dimension %d unsupported", a.d_pad);
     return DRPT_ERR_UNSUPPORTED;
   }
-  k_tile_plan<<<1, 1024, 0, s>>>(a.goff, a.nleaf, a.tile_leaf, a.tile_r0, a.n_tiles);
+  k_tile_plan<<<1, 1024, 0, s>>>(a.goff, a.nleaf, kTM, a.tile_leaf, a.tile_r0, a.n_tiles);
   DRPT_LAUNCH_CHECK();
   CUtensorMap tmA;
   DRPT_TRY(make_tmap(&tmA, a.Xb, a.n, a.d_pad, kTM, a.fp8));
@@ -1294,6 +1291,27 @@ drpt_status launch_leaf_mma(const MixedTreeArgs &a, cudaStream_t s) {
   if (a.kp == 32) return mma_kp<32>(a, tmA, kb, s);
   set_error("mixed leaf kernel: %d candidates per tree unsupported (16 or 32)", a.kp);
   return DRPT_ERR_UNSUPPORTED;
+}
+
+drpt_status launch_tile_plan(const int32_t *goff, int nleaf, int rows, int32_t *tile_leaf,
+                             int32_t *tile_r0, int32_t *n_tiles, cudaStream_t s) {
+  k_tile_plan<<<1, 1024, 0, s>>>(goff, nleaf, rows, tile_leaf, tile_r0, n_tiles);
+  DRPT_LAUNCH_CHECK();
+  return DRPT_OK;
+}
+
+drpt_status launch_fold_lists(const MixedTreeArgs &a, cudaStream_t s) {
+  const unsigned grid = (unsigned)ceil_div(a.n, 256);
+  if (a.kp == 16)
+    k_fold_lists<16><<<grid, 256, 0, s>>>(a.tree_dist, a.tree_idx, a.n, a.cand_dist, a.cand_idx);
+  else if (a.kp == 32)
+    k_fold_lists<32><<<grid, 256, 0, s>>>(a.tree_dist, a.tree_idx, a.n, a.cand_dist, a.cand_idx);
+  else {
+    set_error("fold: %d candidates per tree unsupported (16 or 32)", a.kp);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  DRPT_LAUNCH_CHECK();
+  return DRPT_OK;
 }
 
 drpt_status launch_rerank(const void *X, int dtype, int d, const int32_t *visit, int64_t n,

@@ -138,6 +138,17 @@ int mixed_stage_trees(int64_t n, int d_pad, int fp8, int T);
 drpt_status launch_localize(int32_t *idx, int64_t n, int k, const int64_t *set_off, int nsets,
                             cudaStream_t s);
 drpt_status launch_leaf_mma(const MixedTreeArgs &a, cudaStream_t s);
+// Row tiles of `rows` rows of every leaf (tile_leaf, tile_r0, *n_tiles).
+drpt_status launch_tile_plan(const int32_t *goff, int nleaf, int rows, int32_t *tile_leaf,
+                             int32_t *tile_r0, int32_t *n_tiles, cudaStream_t s);
+// Folds a.tree_idx / a.tree_dist (this tree's lists) into the running list.
+drpt_status launch_fold_lists(const MixedTreeArgs &a, cudaStream_t s);
+// FP32 CUDA-core form of the leaf phase (k_fp32gram.cu): ||x||^2 of every
+// row, then per tree the Gram tiles of whole leaves in FP32 (a.X rows, not
+// staged) into the running list as launch_leaf_mma does.
+drpt_status launch_row_norms(const void *X, int dtype, int64_t n, int d, float *out,
+                             cudaStream_t s);
+drpt_status launch_leaf_f32(const MixedTreeArgs &a, const float *xnorm, cudaStream_t s);
 drpt_status launch_rerank(const void *X, int dtype, int d, const int32_t *visit, int64_t n,
                           const int32_t *cand, int K2, int k, int32_t *out_idx, float *out_dist,
                           cudaStream_t s);

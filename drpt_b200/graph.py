@@ -95,7 +95,7 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
         seeds_arr = (ctypes.c_uint32 * ntrees)(*[int(s) & 0xFFFFFFFF for s in local_seeds])
         desc.local_seeds = seeds_arr
     desc.mode = {"exact": _lib.MODE_EXACT, "fast": _lib.MODE_FAST, "mixed": _lib.MODE_MIXED,
-                 "fp32_leaf": _lib.MODE_FP32_LEAF}[mode]
+                 "fp32_leaf": _lib.MODE_FP32_LEAF, "fp32_gram": _lib.MODE_FP32_GRAM}[mode]
     desc.leaf_size = leaf_size
     desc.precision = {"bf16": _lib.PRECISION_BF16, "fp8": _lib.PRECISION_FP8_E4M3}[precision]
     desc.learned_trees, desc.learn_sample = learned_trees, learn_sample

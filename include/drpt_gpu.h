@@ -73,7 +73,13 @@ typedef enum {
    * global leaves, brute-forced with the exact sequential FP32 distance of
    * the plain form on the CUDA cores (no tensor cores, no re-rank).  The
    * equal-recall FP32 counterpart of DRPT_MODE_MIXED. */
-  DRPT_MODE_FP32_LEAF = 3
+  DRPT_MODE_FP32_LEAF = 3,
+  /* The mixed form with its leaf Gram tiles in FP32 on the CUDA cores:
+   * ||y||^2 - 2 x.y by fused multiply-adds (one per dimension and pair) over
+   * the unstaged rows, the same candidates per point and tree, running list,
+   * FP32 re-rank and FP64 boundary check.  The fastest plain FP32
+   * counterpart of DRPT_MODE_MIXED.  d a multiple of 8, no learned trees. */
+  DRPT_MODE_FP32_GRAM = 4
 } drpt_mode;
 
 /* Operand type of the mixed form's tensor-core leaf tiles (FP32 accumulation

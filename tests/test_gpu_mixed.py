@@ -167,3 +167,33 @@ def test_mixed_fp8_low_dimension(torch, clustered):
     I, D = idx.cpu().numpy(), dist.cpu().numpy()
     for p in q[:10]:
         assert _close(D[p, 0], X[p], X[I[p, 0]])
+
+
+def test_fp32_gram_form_matches_the_fp32_whole_leaf_recall(torch, clustered):
+    """The FP32 CUDA-core Gram form (||y||^2 - 2 x.y by FFMA, re-ranked in
+    exact FP32) on the mixed form's trees: recall within 0.005 of the same
+    trees brute-forced with the exact per-pair FP32 distance, FP32 output
+    distances, no self and no duplicates."""
+    X, Xd = clustered
+    q = recall.sample_queries(len(X), 400, seed=3)
+    ti, _ = recall.exact_knn_fp64(Xd, q, 10)
+    gi, gd, _ = build_graph(Xd, 6, 10, 99, mode="fp32_gram", leaf_size=1024)
+    li, _, _ = build_graph(Xd, 6, 10, 99, mode="fp32_leaf", leaf_size=1024)
+    torch.cuda.synchronize()
+    G, D, Lx = gi.cpu().numpy(), gd.cpu().numpy(), li.cpu().numpy()
+    rg, rl = recall.recall_at_k(G[q], ti), recall.recall_at_k(Lx[q], ti)
+    assert abs(rg - rl) <= 0.005, (rg, rl)
+    assert not (G == np.arange(len(X))[:, None]).any() and (G >= 0).all()
+    assert ((D[:, 1:] >= D[:, :-1])).all()
+    for p in q[:25]:
+        assert len(np.unique(G[p])) == G.shape[1]
+        for j in range(0, 10, 3):
+            assert _close(D[p, j], X[p], X[G[p, j]])
+    # u8 rows (784 dimensions) and 32 candidates per tree
+    U = synth.clustered_u8(8_000, 784, sigma_p=40.0, seed=7)
+    ui, ud, _ = build_graph(U, 3, 16, 5, mode="fp32_gram", leaf_size=512)
+    qu = np.arange(0, len(U), 97)
+    tu, _ = oracle.exact_knn(U, qu, 16)
+    assert recall.recall_at_k(ui[qu], tu) >= 0.8
+    for p in qu[:10]:
+        assert _close(ud[p, 0], U[p], U[ui[p, 0]])
