@@ -44,7 +44,8 @@ def build_lib(reference_root: str | None = None) -> None:
     """Compile libdrpt_oracle.so with the recipe in oracle/Makefile and, when
     a reference checkout is named (`reference_root`, else the environment's
     DRPT_REFERENCE_ROOT), the reference binary _ref/drpt_ref from its
-    sources.  A named root that is not a directory is an error; with none
+    sources and, once libdrpt_gpu.so exists, the reference-side binding's
+    test driver _ref/adapter_check.  A named root that is not a directory is an error; with none
     named the reference binary is not built."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
     root = reference_root or os.environ.get("DRPT_REFERENCE_ROOT")
@@ -53,6 +54,9 @@ def build_lib(reference_root: str | None = None) -> None:
     if not os.path.isdir(root):
         raise FileNotFoundError(f"reference checkout {root!r} (DRPT_REFERENCE_ROOT) not found")
     subprocess.run(["make", "-s", "-C", HERE, "ref", "REF_ROOT=" + root], check=True)
+    # the reference-side binding of the library, where the library is built
+    if os.path.exists(os.path.join(os.path.dirname(HERE), "drpt_b200", "libdrpt_gpu.so")):
+        subprocess.run(["make", "-s", "-C", HERE, "adapter", "REF_ROOT=" + root], check=True)
 
 
 def lib():
