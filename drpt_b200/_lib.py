@@ -28,8 +28,9 @@ EXPORTS = [
     "drpt_host_projection", "drpt_project", "drpt_global_trees", "drpt_local_leaves",
     "drpt_leaf_knn", "drpt_merge_candidates", "drpt_global_trees_noalloc",
     "drpt_build_graph_batched", "drpt_learn_gradient", "drpt_index_build", "drpt_index_query",
-    "drpt_index_destroy", "drpt_locality_slots", "drpt_build_graph_stream",
+    "drpt_index_destroy", "drpt_locality_slots", "drpt_build_graph_stream", "drpt_project_sign",
 ]
+PROJECTION_GAUSSIAN, PROJECTION_SIGN = 0, 1
 
 
 class DrptError(RuntimeError):
@@ -52,7 +53,7 @@ class BuildDesc(ctypes.Structure):
         ("stream", ctypes.c_void_p), ("leaf_size", ctypes.c_int32), ("precision", ctypes.c_int32),
         ("learned_trees", ctypes.c_int32), ("learn_sample", ctypes.c_int32),
         ("learn_iters", ctypes.c_int32), ("locality", ctypes.c_int32),
-        ("list_width", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("list_width", ctypes.c_int32), ("projection", ctypes.c_int32),
     ]
 
 
@@ -115,6 +116,7 @@ def load(path: str = LIB_PATH):
                                               ctypes.POINTER(vp), ctypes.POINTER(Stats)]
         L.drpt_host_projection.argtypes = [u32, i32, i32, ctypes.c_float, vp]
         L.drpt_project.argtypes = [vp, vp, i64, i32, i32, vp, i32, vp, i32, vp, vp]
+        L.drpt_project_sign.argtypes = [vp, vp, i64, i32, vp, i32, vp, i32, vp, vp]
         L.drpt_global_trees.argtypes = [vp, vp, i64, i32, i32, i32, vp, vp, vp, vp]
         L.drpt_local_leaves.argtypes = [vp, vp, vp, i64, i32, i32, i32, vp, vp, vp]
         L.drpt_locality_slots.argtypes = [vp, vp, i64, i32, i32, vp, vp, vp]

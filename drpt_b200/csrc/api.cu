@@ -180,6 +180,64 @@ drpt_status project_cols(drpt_ctx *c, const void *X, int dtype, int64_t n, int d
   return DRPT_OK;
 }
 
+// The sign-matrix projection of u8 rows (K1u, a fast form): S = sign of the
+// projection matrix's selected columns (the same sparsity mask), P = X.S^T
+// exactly in integers on the tensor cores, at most project_i8_max_cols()
+// columns per launch.  Also leaves the signs as the CSC an index keeps
+// (csc_*), so that out-of-sample queries project the same way.
+drpt_status project_sign(drpt_ctx *c, const void *X, int64_t n, int d, const float *B, int L,
+                         const std::vector<int32_t> &cols, float *P, cudaStream_t s,
+                         int *nnz_out = nullptr) {
+  const int ncols = (int)cols.size();
+  if (d % 16 != 0) {
+    set_error("the sign-matrix projection needs d %% 16 == 0 (got %d)", d);
+    return DRPT_ERR_UNSUPPORTED;
+  }
+  const int per = project_i8_max_cols();
+  std::vector<int32_t> colptr(ncols + 1, 0), row;
+  std::vector<float> val;
+  const int groups = (ncols + per - 1) / per;
+  std::vector<int8_t> S((size_t)groups * per * d, 0);  // per group: `per` rows of d signs
+  for (int q = 0; q < ncols; ++q) {
+    int8_t *srow = S.data() + ((size_t)(q / per) * per + q % per) * d;
+    for (int k = 0; k < d; ++k) {
+      const float b = B[(int64_t)k * L + cols[q]];
+      if (b != 0.0f) {
+        const int8_t sg = b > 0.0f ? 1 : -1;
+        srow[k] = sg;
+        row.push_back(k);
+        val.push_back((float)sg);
+      }
+    }
+    colptr[q + 1] = (int32_t)row.size();
+  }
+  int32_t *dcol, *drow;
+  float *dval;
+  int8_t *dS;
+  int *err;
+  DRPT_TRY(ws_get(c, "csc_colptr", colptr.size(), &dcol));
+  DRPT_TRY(ws_get(c, "csc_row", std::max<size_t>(row.size(), 1), &drow));
+  DRPT_TRY(ws_get(c, "csc_val", std::max<size_t>(val.size(), 1), &dval));
+  DRPT_TRY(ws_get(c, "sgn_S", S.size(), &dS));
+  DRPT_TRY(ws_get(c, "sgn_err", 1, &err));
+  // Pageable sources: the copies complete before these calls return.
+  DRPT_CUDA(cudaMemcpyAsync(dcol, colptr.data(), colptr.size() * 4, cudaMemcpyHostToDevice, s));
+  if (!row.empty()) {
+    DRPT_CUDA(cudaMemcpyAsync(drow, row.data(), row.size() * 4, cudaMemcpyHostToDevice, s));
+    DRPT_CUDA(cudaMemcpyAsync(dval, val.data(), val.size() * 4, cudaMemcpyHostToDevice, s));
+  }
+  DRPT_CUDA(cudaMemcpyAsync(dS, S.data(), S.size(), cudaMemcpyHostToDevice, s));
+  DRPT_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  if (nnz_out) *nnz_out = (int)row.size();
+  for (int g = 0; g < groups; ++g) {
+    const int nc = std::min(per, ncols - g * per);
+    DRPT_TRY(launch_project_i8(static_cast<const uint8_t *>(X), n, d, dS + (size_t)g * per * d,
+                               nc, P + (size_t)g * per * n, err, s));
+    c->launches += 1;
+  }
+  return DRPT_OK;
+}
+
 // Global trees of all T trees; returns pointers to the final order/offsets
 // (inside the workspace).
 drpt_status global_trees(drpt_ctx *c, const float *P, int64_t n, int T, int gd, int exact,
@@ -564,9 +622,13 @@ void leaf_phase_ms(drpt_ctx *c, float *stage, float *mma) {
 drpt_status mixed_check(drpt_ctx *c, cudaStream_t s) {
   int *err_d = nullptr;
   DRPT_TRY(ws_get(c, "mx_err", 1, &err_d));
-  int err = 0;
+  int err = 0, serr = 0;
   DRPT_CUDA(cudaMemcpyAsync(&err, err_d, sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (c->bufs.count("sgn_err")) {  // the sign-matrix projection's bounded waits
+    DRPT_CUDA(cudaMemcpyAsync(&serr, c->bufs["sgn_err"].p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  }
   DRPT_CUDA(cudaStreamSynchronize(s));
+  if (serr) err |= 1;
   if (err & 2) {
     set_error("a global leaf holds more than 8192 points (the tensor-core leaf kernel's limit); "
               "use a smaller leaf_size");
@@ -937,8 +999,18 @@ drpt_status run_mixed(drpt_ctx *c, const drpt_build_desc *desc, const void *X, i
   float *P = nullptr;
   DRPT_TRY(ws_get(c, "P", std::max<size_t>((size_t)T * (gd - 1), 1) * n, &P));
   int nnz = 0;
-  if (!cols.empty())
+  if (desc->projection == DRPT_PROJECTION_SIGN) {
+    if (desc->dtype != DRPT_DTYPE_U8) {
+      set_error("the sign-matrix projection takes u8 rows");
+      return DRPT_ERR_UNSUPPORTED;
+    }
+    if (!cols.empty()) DRPT_TRY(project_sign(c, X, n, d, B.data(), L, cols, P, s, &nnz));
+  } else if (desc->projection != DRPT_PROJECTION_GAUSSIAN) {
+    set_error("unknown projection %d", desc->projection);
+    return DRPT_ERR_INVALID_ARG;
+  } else if (!cols.empty()) {
     DRPT_TRY(project_cols(c, X, desc->dtype, n, d, B.data(), L, cols, P, s, &nnz));
+  }
   LearnResult lres;
   float ms_learn = 0.0f;
   if (learned > 0) {
@@ -1640,6 +1712,11 @@ static drpt_status build_graph_impl(drpt_ctx *c, const drpt_build_desc *desc, co
     X = xd;
   }
 
+  if (desc->projection != DRPT_PROJECTION_GAUSSIAN && desc->mode != DRPT_MODE_MIXED &&
+      desc->mode != DRPT_MODE_FP32_GRAM) {
+    set_error("the sign-matrix projection is an option of the mixed and FP32 Gram forms only");
+    return DRPT_ERR_INVALID_ARG;
+  }
   if (desc->mode == DRPT_MODE_MIXED || desc->mode == DRPT_MODE_FP32_LEAF ||
       desc->mode == DRPT_MODE_FP32_GRAM) {
     int32_t *oi = out_idx;
@@ -2010,6 +2087,32 @@ drpt_status drpt_project(drpt_ctx *c, const void *X, int64_t n, int32_t d, int32
   DRPT_CUDA(cudaSetDevice(c->device));
   std::vector<int32_t> cols(cols_host, cols_host + ncols);
   return project_cols(c, X, dtype, n, d, B_host, L, cols, P, (cudaStream_t)stream);
+}
+
+drpt_status drpt_project_sign(drpt_ctx *c, const uint8_t *X, int64_t n, int32_t d,
+                              const float *B_host, int32_t L, const int32_t *cols_host,
+                              int32_t ncols, float *P, void *stream) {
+  if (!c || !X || !B_host || !cols_host || !P || n <= 0 || d <= 0 || L <= 0 || ncols <= 0) {
+    set_error("drpt_project_sign: null pointer or empty size");
+    return DRPT_ERR_INVALID_ARG;
+  }
+  for (int q = 0; q < ncols; ++q)
+    if (cols_host[q] < 0 || cols_host[q] >= L) {
+      set_error("drpt_project_sign: column %d outside [0, %d)", cols_host[q], L);
+      return DRPT_ERR_INVALID_ARG;
+    }
+  DRPT_CUDA(cudaSetDevice(c->device));
+  std::vector<int32_t> cols(cols_host, cols_host + ncols);
+  const cudaStream_t s = (cudaStream_t)stream;
+  DRPT_TRY(project_sign(c, X, n, d, B_host, L, cols, P, s));
+  int serr = 0;
+  DRPT_CUDA(cudaMemcpyAsync(&serr, c->bufs["sgn_err"].p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DRPT_CUDA(cudaStreamSynchronize(s));
+  if (serr) {
+    set_error("a bounded wait in the sign-matrix projection gave up");
+    return DRPT_ERR_TIMEOUT;
+  }
+  return DRPT_OK;
 }
 
 drpt_status drpt_global_trees(drpt_ctx *c, const float *P, int64_t n, int32_t T, int32_t gd,

@@ -28,7 +28,8 @@
 //      -data-set-size (the reference ignores it).
 // Sizes are checked against the file; a short file is an error.
 //
-// Further flags: -precision bf16|fp8 and -learned-trees N (mixed form),
+// Further flags: -precision bf16|fp8, -projection gaussian|sign (u8 rows) and
+// -learned-trees N (mixed form),
 // -write-distances 1 (a third column: the neighbour's Euclidean distance).
 
 #include <drpt_gpu.h>
@@ -58,6 +59,7 @@ struct Options {
   uint32_t seed = 0;
   int mode = DRPT_MODE_EXACT;
   int precision = DRPT_PRECISION_BF16;
+  int projection = DRPT_PROJECTION_GAUSSIAN;
   int learned_trees = 0;
   int locality = 0;
   bool write_distances = false;
@@ -103,6 +105,10 @@ Options parse(int argc, char **argv) {
       if (!std::strcmp(v, "bf16")) o.precision = DRPT_PRECISION_BF16;
       else if (!std::strcmp(v, "fp8")) o.precision = DRPT_PRECISION_FP8_E4M3;
       else die("-precision must be bf16 or fp8");
+    } else if (!std::strcmp(f, "-projection")) {
+      if (!std::strcmp(v, "gaussian")) o.projection = DRPT_PROJECTION_GAUSSIAN;
+      else if (!std::strcmp(v, "sign")) o.projection = DRPT_PROJECTION_SIGN;
+      else die("-projection must be gaussian or sign");
     } else if (!std::strcmp(f, "-learned-trees")) o.learned_trees = std::atoi(v);
     else if (!std::strcmp(f, "-write-distances")) o.write_distances = std::atoi(v) == 1;
   }
@@ -251,6 +257,7 @@ int main(int argc, char **argv) {
   desc.mode = o.mode;
   desc.leaf_size = o.leaf_size;
   desc.precision = o.precision;
+  desc.projection = o.projection;
   desc.learned_trees = o.learned_trees;
   desc.locality = o.locality;
   std::vector<int32_t> idx((size_t)o.n * o.nn);

@@ -138,6 +138,12 @@ int mixed_stage_trees(int64_t n, int d_pad, int fp8, int T);
 drpt_status launch_localize(int32_t *idx, int64_t n, int k, const int64_t *set_off, int nsets,
                             cudaStream_t s);
 drpt_status launch_leaf_mma(const MixedTreeArgs &a, cudaStream_t s);
+// K1u (k_project_i8.cu): P (nc x n, column-major) = X (n x d u8) . S^T with S
+// (ncp x d signed bytes, ncp = nc rounded up to 16, extra rows zero) on the
+// tensor cores in s32; d % 16 == 0, nc <= project_i8_max_cols().
+int project_i8_max_cols();
+drpt_status launch_project_i8(const uint8_t *X, int64_t n, int d, const int8_t *S, int nc,
+                              float *P, int *err, cudaStream_t s);
 // Row tiles of `rows` rows of every leaf (tile_leaf, tile_r0, *n_tiles).
 drpt_status launch_tile_plan(const int32_t *goff, int nleaf, int rows, int32_t *tile_leaf,
                              int32_t *tile_r0, int32_t *n_tiles, cudaStream_t s);

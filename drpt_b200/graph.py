@@ -63,7 +63,7 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
                 density: float = 0.0, local_seeds=None, device: int = 0, stream=None,
                 out=None, leaf_size: int = 0, precision: str = "bf16", learned_trees: int = 0,
                 learn_sample: int = 0, learn_iters: int = 0, locality: bool = False,
-                list_width: int = 0, _index_out=None):
+                list_width: int = 0, projection: str = "gaussian", _index_out=None):
     """k-NN graph of `data` (n x d, uint8 or float32; a NumPy array in host
     memory or a CUDA tensor).  Returns (idx, dist, stats): idx int32 and dist
     float32 of shape (n, nn), each point's nn nearest distinct neighbours other
@@ -77,7 +77,10 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
     reference's locality relabelling of the global leaves; at one rank the
     graph is the same either way.  `list_width` (mixed mode: 16 or 32, at
     least nn; 0 = 16 for nn <= 10, else 32) is how many candidates per point
-    and tree the mixed form keeps for its final FP32 re-rank."""
+    and tree the mixed form keeps for its final FP32 re-rank.  `projection`
+    ("gaussian" or "sign"; mixed and fp32_gram modes, uint8 rows with d a
+    multiple of 16): "sign" projects with the sign of the reference's sparse
+    Gaussian matrix as an exact integer product on the tensor cores."""
     on_dev = _is_cuda_tensor(data)
     if not on_dev:
         data = np.ascontiguousarray(data)
@@ -102,6 +105,7 @@ def build_graph(data, ntrees: int, nn: int, seed: int, *, mode: str = "exact",
     desc.learn_iters = learn_iters
     desc.locality = 1 if locality else 0
     desc.list_width = list_width
+    desc.projection = {"gaussian": _lib.PROJECTION_GAUSSIAN, "sign": _lib.PROJECTION_SIGN}[projection]
     desc.data_on_device = 1 if on_dev else 0
     desc.out_on_device = desc.data_on_device
     if on_dev:

@@ -92,6 +92,16 @@ typedef enum {
 
 typedef struct drpt_ctx drpt_ctx;
 
+typedef enum {
+  /* The reference's sparse Gaussian matrix in FP32 (every mode). */
+  DRPT_PROJECTION_GAUSSIAN = 0,
+  /* Its sign (+1 / -1 where it is non-zero, the same sparsity mask) applied
+   * to u8 rows as an exact u8 x s8 -> s32 product on the tensor cores
+   * (tcgen05.mma kind::i8); d a multiple of 16.  A fast form: the trees are
+   * not the reference's and are judged by recall. */
+  DRPT_PROJECTION_SIGN = 1
+} drpt_projection;
+
 typedef struct {
   int64_t n;                  /* points */
   int32_t d;                  /* dimensions */
@@ -128,7 +138,8 @@ typedef struct {
   int32_t list_width;         /* mixed mode: candidates kept per point and tree
                                  for the final re-rank, 16 or 32 and >= nn
                                  (0 = 16 for nn <= 10, else 32) */
-  int32_t reserved;
+  int32_t projection;         /* drpt_projection: mixed and FP32 Gram forms may
+                                 project u8 rows with the sign matrix */
 } drpt_build_desc;
 
 typedef struct {
@@ -273,6 +284,16 @@ drpt_status drpt_host_projection(uint32_t seed, int32_t d, int32_t L, float dens
 drpt_status drpt_project(drpt_ctx *ctx, const void *X, int64_t n, int32_t d, int32_t dtype,
                          const float *B_host, int32_t L, const int32_t *cols_host,
                          int32_t ncols, float *P, void *stream);
+
+/* The sign-matrix projection (no reference counterpart; the fast form of
+ * MathOp::multiply_mat for u8 rows): P[c][i] = sum_k X[i][k] * sign(B[k][col(c)])
+ * over the non-zero entries, exact in 32-bit integers on the tensor cores
+ * (tcgen05.mma kind::i8) and stored as float; X is u8 (n x d, d % 16 == 0)
+ * on the device, P column-major (ncols x n).  Synchronises the stream to
+ * read the kernel's error flag. */
+drpt_status drpt_project_sign(drpt_ctx *ctx, const uint8_t *X, int64_t n, int32_t d,
+                              const float *B_host, int32_t L, const int32_t *cols_host,
+                              int32_t ncols, float *P, void *stream);
 
 /* Global trees of all T trees from the projected columns P (column t*(gd-1)
  * + level, n values each).  order (T x n): point ids grouped by global leaf in
