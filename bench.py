@@ -393,11 +393,12 @@ def other_workload(args):
         # level (recall 0.840 against 0.844 with 10 steps, at half the training)
         sample, iters = (50_000, 3) if lt else (0, 0)
 
-        def run(mode="mixed", trees=T, precision=prec, learned=lt, out=(idx, dst), smp=sample):
+        def run(mode="mixed", trees=T, precision=prec, learned=lt, out=(idx, dst), smp=sample,
+                projection="gaussian"):
             return build_graph(Xd, trees, nn, SEED_PROJ, mode=mode, leaf_size=leaf,
                                precision=precision, learned_trees=learned, out=out,
                                learn_sample=smp if learned else 0,
-                               learn_iters=iters if learned else 0)[2]
+                               learn_iters=iters if learned else 0, projection=projection)[2]
         for _ in range(warm):
             run()
         with ClockSampler(0) as clocks:
@@ -419,18 +420,28 @@ def other_workload(args):
         others = []
         if wl == "fbin-2m-960":
             others.append(("mixed_bf16", dict(precision="bf16")))
+        if wl == "ubyte-60k-784":
+            # the u8 rows projected with the sign matrix on the tensor cores
+            others.append(("mixed_sign_projection", dict(projection="sign")))
         if lt:
             others += [("mixed_learned_sample_8192", dict(smp=8192)),
                        (f"mixed_{T}_random_trees", dict(learned=0)),
                        (f"mixed_{2 * T}_random_trees", dict(trees=2 * T, learned=0)),
                        (f"fp32_leaf_{2 * T}_random_trees", dict(mode="fp32_leaf", trees=2 * T,
+                                                                  learned=0)),
+                       (f"fp32_gram_{2 * T}_random_trees", dict(mode="fp32_gram", trees=2 * T,
                                                                   learned=0))]
         else:
             others.append((f"fp32_leaf_{T}_trees", dict(mode="fp32_leaf")))
+            others.append((f"fp32_gram_{T}_trees", dict(mode="fp32_gram")))
         for name, kw in others:
-            _, pms = _timed(lambda: run(out=(pi, pd), **kw), 1)
+            pst, pms = _timed(lambda: run(out=(pi, pd), **kw), 1)
             comps[name] = {"points_per_s": n / (pms / 1e3), "ms": pms,
                            "recall@10": rec_of(pi, q, ti, 10)}
+            if kw.get("projection") == "sign":
+                # projection and tree levels, against the Gaussian build's
+                comps[name]["global_ms"] = pst.ms_global
+                comps[name]["global_ms_gaussian"] = st.ms_global
         eq = [v for k, v in comps.items() if k.startswith("fp32") and v["recall@10"] >= rec - 0.01]
         comps["mixed_over_plain_fp32_at_equal_recall"] = \
             min(v["ms"] for v in eq) / ms if eq else None
@@ -478,6 +489,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain-compare", action="store_true")
+    ap.add_argument("--points", type=int, default=0,
+                    help="profiling cases only: this many points of the main workload's "
+                         "distribution (clusters scaled alike) instead of 1,000,000")
     ap.add_argument("--workload", default="fbin-1m-128",
                     choices=["fbin-1m-128", "ubyte-60k-784", "fbin-2m-960", "batch-256x96",
                              "learned-1m-256"])
@@ -488,6 +502,13 @@ def main():
     if args.workload != "fbin-1m-128":
         other_workload(args)
         return
+    global N_POINTS, N_CLUSTERS, WORKLOAD
+    if args.points:
+        # a smaller case of the same distribution, for profiling only
+        N_CLUSTERS = max(1, round(N_CLUSTERS * args.points / N_POINTS))
+        N_POINTS = args.points
+        WORKLOAD = WORKLOAD.replace("1,000,000", f"{N_POINTS:,}").replace(
+            "1000 Gaussian", f"{N_CLUSTERS} Gaussian") + " (profiling case)"
 
     import torch
     import torch.distributed as dist
