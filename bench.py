@@ -370,19 +370,25 @@ def other_workload(args):
         launches = st.kernels_launched * steps
         roof = None
     else:
+        # --points: a smaller case of the same distribution, for profiling only
+        pts = args.points
         if wl == "ubyte-60k-784":
-            X = synth.clustered_u8(60_000, 784, seed=1)
+            X = synth.clustered_u8(pts or 60_000, 784, seed=1)
             nn, T, leaf, prec, lt = 10, 12, 1024, "bf16", 0
             desc = "60,000 x 784 uint8 (IDX3-shaped), 10 centres with 80% zero coordinates, sigma 20"
         elif wl == "fbin-2m-960":
-            X = synth.anisotropic_f32(2_000_000, 960, n_clusters=500, seed=3)
+            X = synth.anisotropic_f32(pts or 2_000_000, 960,
+                                      n_clusters=max(1, round(500 * (pts or 2_000_000) / 2e6)),
+                                      seed=3)
             nn, T, leaf, prec, lt = 20, 32, 2048, "fp8", 0
             desc = ("2,000,000 x 960 float32, 500 anisotropic Gaussians (per-dim sigma U[0.01,0.3]), "
                     "values in [0,1]")
         else:
-            X = synth.latent_manifold_f32(1_000_000, 256, seed=5)
+            X = synth.latent_manifold_f32(pts or 1_000_000, 256, seed=5)
             nn, T, leaf, prec, lt = 10, 16, 1024, "bf16", 8
             desc = "1,000,000 x 256 float32, x = tanh(A z + b) * 4 + N(0, 0.05^2), z ~ N(0, I_16)"
+        if pts:
+            desc = f"{pts:,}-point profiling case of: " + desc
         n, d = X.shape
         Xd = torch.from_numpy(X).cuda()
         del X
