@@ -466,6 +466,17 @@ __device__ __forceinline__ void key_merge_into(float *L, const float *S) {
     }
 }
 
+// L (ascending, N) <- the N smallest of L and `key`: one compare-exchange sweep.
+template <int N>
+__device__ __forceinline__ void key_insert(float *L, float key) {
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const float lo = fminf(L[i], key);
+    key = fmaxf(L[i], key);
+    L[i] = lo;
+  }
+}
+
 // Shared-memory layout.  Every operand tile is rows of 128 bytes (64 BF16 or
 // 128 E4M3 values of one 128-byte K block), 128-byte swizzled, 1024-byte
 // aligned.
@@ -700,9 +711,15 @@ __global__ void __launch_bounds__(MmaCfg<KP, STREAM>::threads,
     constexpr int kChains = 2, kLane = kBufSlots / kChains, kPerBatch = 16 / kChains;
     uint32_t *const pbase = buf + grp * kBufSlots * kTM + row;
     const uint32_t abase = smem_u32(pbase);
-    uint32_t aslot[kChains];
+    uint32_t aslot[kChains], alim[kChains];
 #pragma unroll
-    for (int q = 0; q < kChains; ++q) aslot[q] = abase + q * kLane * kTM * 4;
+    for (int q = 0; q < kChains; ++q) {
+      aslot[q] = abase + q * kLane * kTM * 4;
+      // after a check that does not flush a chain holds at most
+      // kLane - kCheck / kChains keys, so the next kCheck / kChains stores
+      // stay inside its kLane slots
+      alim[q] = aslot[q] + (kLane - kCheck / kChains) * kTM * 4;
+    }
     auto pending = [&](int q) {
       return (int)((aslot[q] - abase - q * kLane * kTM * 4) / (kTM * 4));
     };
@@ -714,7 +731,20 @@ __global__ void __launch_bounds__(MmaCfg<KP, STREAM>::threads,
         mine = max(mine, cnt[q]);
       }
       const int mx = __reduce_max_sync(kFull, mine);
-      for (int base = 0; base < mx; base += kPerBatch) {
+      if (mx <= 3) {
+        // few pending keys (the common case once a threshold is set): insert
+        // them one by one (2 KP min/max each) rather than sort a batch of 16
+        // and merge it (about 240); the kept keys are the same
+#pragma unroll
+        for (int q = 0; q < kChains; ++q)
+          for (int slot = 0; slot < mx; ++slot) {
+            uint32_t key = 0x7f800000u;
+            if (slot < cnt[q]) key = pbase[(q * kLane + slot) * kTM];
+            if ((key & kColMask) == my_col && key != 0x7f800000u) key = 0x7f800000u;
+            key_insert<KP>(td, __uint_as_float(key));
+          }
+      }
+      for (int base = 0; mx > 3 && base < mx; base += kPerBatch) {
         float sd[16];
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
@@ -783,13 +813,10 @@ __global__ void __launch_bounds__(MmaCfg<KP, STREAM>::threads,
           else sv = fmaf(-2.0f, v[j], nc[e]);
           append(aslot[j % kChains], sv, nc[e]);
         }
-        int most = 0;
+        bool over = false;
 #pragma unroll
-        for (int q = 0; q < kChains; ++q) most = max(most, pending(q));
-        // after a check that does not flush a chain holds at most
-        // kLane - kCheck / kChains keys, so the next kCheck / kChains
-        // stores stay inside its kLane slots
-        if (__any_sync(kFull, most > kLane - kCheck / kChains)) flush();
+        for (int q = 0; q < kChains; ++q) over |= aslot[q] > alim[q];
+        if (__any_sync(kFull, over)) flush();
       }
     };
     const uint32_t lane_base = tmem + ((uint32_t)(wq * 32) << 16);

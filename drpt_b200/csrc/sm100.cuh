@@ -39,12 +39,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// The same with a suspend-time hint: a waiting thread sleeps up to `ns`
+// nanoseconds per try (it wakes when the phase completes), so a long wait
+// issues few instructions next to the warps that do the work.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
 // Bounded wait: gives up after about `limit_cycles` and returns false.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
                                           long long limit_cycles = 4000000000LL) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity)) {
+  while (!mbar_try_wait_sleep(bar, parity, 1000u)) {
     if (clock64() - t0 > limit_cycles) return false;
   }
   return true;
