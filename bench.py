@@ -433,6 +433,10 @@ def other_workload(args):
             others += [("mixed_learned_sample_8192", dict(smp=8192)),
                        (f"mixed_{T}_random_trees", dict(learned=0)),
                        (f"mixed_{2 * T}_random_trees", dict(trees=2 * T, learned=0)),
+                       # a learned configuration past recall 0.90, and random
+                       # trees to meet it
+                       (f"mixed_{T}_random_{T}_learned_trees", dict(trees=2 * T, learned=T)),
+                       (f"mixed_{3 * T}_random_trees", dict(trees=3 * T, learned=0)),
                        (f"fp32_leaf_{2 * T}_random_trees", dict(mode="fp32_leaf", trees=2 * T,
                                                                   learned=0)),
                        (f"fp32_gram_{2 * T}_random_trees", dict(mode="fp32_gram", trees=2 * T,
