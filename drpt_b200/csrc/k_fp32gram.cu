@@ -32,9 +32,9 @@ constexpr int kCols = 128;       // columns per tile
 constexpr int kKc = 32;          // dimensions per staged chunk
 constexpr int kThreads = 256;
 constexpr int kParts = 2;        // threads per row in the selection
-constexpr int kPitch = kCols + 4;  // score-tile row pitch (words)
+constexpr int kPitch = kCols + 2;  // score-tile row pitch (words)
 constexpr int kPool = kRows * kPitch;  // floats of the shared pool
-static_assert(kKc * (kRows + kCols) <= kPool, "staged chunks fit the pool");
+static_assert(2 * kKc * (kRows + kCols) <= kPool, "two buffers of staged chunks fit the pool");
 static_assert(2 * 32 * kRows <= kPool, "a 32-entry hand-over list fits the pool");
 constexpr size_t kSmem = sizeof(float) * (kPool + kCols) + sizeof(int32_t) * kRows;
 constexpr int kMaxLeaf = 1 << 13;  // the mixed form's leaf limit
@@ -84,7 +84,8 @@ __global__ void __launch_bounds__(256) k_row_norms(const T *__restrict__ X, int6
 }
 
 // Ascending list of N (score, column) pairs <- the N smallest of it and
-// (v, c) by (score, column): one compare-exchange sweep.
+// (v, c) by (score, column): one compare-exchange sweep (used to merge two
+// lists, where columns interleave).
 template <int N>
 __device__ __forceinline__ void pair_insert(float *Lv, int32_t *Lc, float v, int32_t c) {
 #pragma unroll
@@ -99,6 +100,24 @@ __device__ __forceinline__ void pair_insert(float *Lv, int32_t *Lc, float v, int
   }
 }
 
+// The same for a (v, c) whose column is above every column in the list (the
+// scan order): entry i becomes entry i - 1 where v < old entry i - 1, (v, c)
+// where it falls between them, else stays; every entry from the old list at
+// once, no chain through (v, c).  Equal scores keep the earlier column.
+template <int N>
+__device__ __forceinline__ void pair_shift_in(float *Lv, int32_t *Lc, float v, int32_t c) {
+  bool below[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) below[i] = v < Lv[i];
+#pragma unroll
+  for (int i = N - 1; i > 0; --i) {
+    Lv[i] = below[i - 1] ? Lv[i - 1] : (below[i] ? v : Lv[i]);
+    Lc[i] = below[i - 1] ? Lc[i - 1] : (below[i] ? c : Lc[i]);
+  }
+  Lv[0] = below[0] ? v : Lv[0];
+  Lc[0] = below[0] ? c : Lc[0];
+}
+
 template <typename T, int KP>
 __global__ void __launch_bounds__(kThreads, 1) k_leaf_f32(
     const T *__restrict__ X, int d, const int32_t *__restrict__ goff,
@@ -108,12 +127,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_leaf_f32(
     float *__restrict__ run_dist, int32_t *__restrict__ tree_idx, float *__restrict__ tree_dist,
     int *err) {
   // One dynamic pool, three uses in turn: the staged chunks (As: rows, Bs:
-  // columns, dimension-major), the tile's scores St (row pitch kPitch, so
-  // that the two threads of a row reading columns 2j + part hit distinct
-  // banks), and at the end the list part 1 hands to part 0.
+  // columns, dimension-major), the tile's scores St (row pitch kPitch = 2
+  // mod 32 words, so that the 16 rows x 2 parts of a warp reading columns
+  // 2j + part hit 32 distinct banks), and at the end the list part 1 hands
+  // to part 0.
   extern __shared__ __align__(16) float pool[];
-  float(*As)[kRows] = reinterpret_cast<float(*)[kRows]>(pool);
-  float(*Bs)[kCols] = reinterpret_cast<float(*)[kCols]>(pool + kKc * kRows);
+  // two buffers of staged chunks: chunk i is used from buffer i & 1 while
+  // chunk i + 1 is stored into the other
+  auto As = [&](int b) { return reinterpret_cast<float(*)[kRows]>(pool + b * kKc * (kRows + kCols)); };
+  auto Bs = [&](int b) {
+    return reinterpret_cast<float(*)[kCols]>(pool + b * kKc * (kRows + kCols) + kKc * kRows);
+  };
   float(*St)[kPitch] = reinterpret_cast<float(*)[kPitch]>(pool);
   float(*hv)[kRows] = reinterpret_cast<float(*)[kRows]>(pool);                 // [KP][row]
   int32_t(*hc)[kRows] = reinterpret_cast<int32_t(*)[kRows]>(pool + KP * kRows);
@@ -152,13 +176,41 @@ __global__ void __launch_bounds__(kThreads, 1) k_leaf_f32(
   // staging: thread takes 16 dimensions of row (or column) tid / 2
   const int sg = tid >> 1, sk = (tid & 1) * 16;
   const int32_t arow = rid[sg];
+  // The next column tile's ids, norm and first chunk are loaded while the
+  // current tile is computed, so that no tile starts on global-memory
+  // latency (the id, then the row it names).
+  auto col_id = [&](int c0, int i) {
+    return c0 < m && i < min(kCols, m - c0) ? __ldg(order + lo + c0 + i) : -1;
+  };
+  float pa[16], pb[16];
+  auto fetch = [&](int32_t bc, int k0) {
+    const T *ra = X + (int64_t)max(arow, 0) * d + k0 + sk;
+    const T *rb = X + (int64_t)max(bc, 0) * d + k0 + sk;
+    load_row8<T>(ra, arow >= 0 && k0 + sk < d, pa);
+    load_row8<T>(ra + 8, arow >= 0 && k0 + sk + 8 < d, pa + 8);
+    load_row8<T>(rb, bc >= 0 && k0 + sk < d, pb);
+    load_row8<T>(rb + 8, bc >= 0 && k0 + sk + 8 < d, pb + 8);
+  };
+  auto store = [&](int b) {
+    float(*A)[kRows] = As(b);
+    float(*B)[kCols] = Bs(b);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      A[sk + e][sg] = pa[e];
+      B[sk + e][sg] = pb[e];
+    }
+  };
+  int32_t bcol = col_id(0, sg);                 // staged column sg of this tile
+  int32_t qn = tid < kCols ? col_id(0, tid) : -1;  // column tid (its norm)
+  float cn = qn >= 0 ? __ldg(xnorm + qn) : __int_as_float(0x7f800000);
+  fetch(bcol, 0);
   for (int c0 = 0; c0 < m; c0 += kCols) {
     const int cols = min(kCols, m - c0);
-    const int32_t bcol = sg < cols ? __ldg(order + lo + c0 + sg) : -1;  // staged column sg
-    if (tid < kCols) {
-      const int32_t q = tid < cols ? __ldg(order + lo + c0 + tid) : -1;   // column tid's norm
-      cnorm[tid] = q >= 0 ? __ldg(xnorm + q) : __int_as_float(0x7f800000);
-    }
+    const int nc0 = c0 + kCols;
+    // the next tile's ids now, its norms a chunk later
+    const int32_t bcol_next = col_id(nc0, sg);
+    const int32_t qn_next = tid < kCols ? col_id(nc0, tid) : -1;
+    float cn_next = __int_as_float(0x7f800000);
     // thread (ty, tx) owns rows 4ty + i and 64 + 4ty + i, columns 4tx + j
     // and 64 + 4tx + j (i, j < 4): conflict-free 16-byte reads of a chunk row
     float acc[8][8];
@@ -166,31 +218,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_leaf_f32(
     for (int i = 0; i < 8; ++i)
 #pragma unroll
       for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
-    float pa[16], pb[16];
-    auto fetch = [&](int k0) {
-      const T *ra = X + (int64_t)max(arow, 0) * d + k0 + sk;
-      const T *rb = X + (int64_t)max(bcol, 0) * d + k0 + sk;
-      load_row8<T>(ra, arow >= 0 && k0 + sk < d, pa);
-      load_row8<T>(ra + 8, arow >= 0 && k0 + sk + 8 < d, pa + 8);
-      load_row8<T>(rb, bcol >= 0 && k0 + sk < d, pb);
-      load_row8<T>(rb + 8, bcol >= 0 && k0 + sk + 8 < d, pb + 8);
-    };
-    fetch(0);
-    for (int k0 = 0; k0 < d; k0 += kKc) {
-      __syncthreads();  // the previous chunk (or tile's scores) is no longer read
-#pragma unroll
-      for (int e = 0; e < 16; ++e) {
-        As[sk + e][sg] = pa[e];
-        Bs[sk + e][sg] = pb[e];
-      }
-      __syncthreads();
-      if (k0 + kKc < d) fetch(k0 + kKc);  // in flight while this chunk is used
+    __syncthreads();  // the previous tile's scores are no longer read
+    if (tid < kCols) cnorm[tid] = cn;
+    store(0);
+    __syncthreads();
+    int cur = 0;
+    for (int k0 = 0; k0 < d; k0 += kKc, cur ^= 1) {
+      const bool more = k0 + kKc < d;
+      // in flight while this chunk is used: the next chunk, or the next
+      // tile's first one
+      if (more) fetch(bcol, k0 + kKc);
+      else if (nc0 < m) fetch(bcol_next, 0);
+      if (k0 == 0 && qn_next >= 0) cn_next = __ldg(xnorm + qn_next);
+      const float(*A)[kRows] = As(cur);
+      const float(*B)[kCols] = Bs(cur);
 #pragma unroll 4
       for (int kk = 0; kk < kKc; ++kk) {
-        const float4 a0 = *reinterpret_cast<const float4 *>(&As[kk][4 * ty]);
-        const float4 a1 = *reinterpret_cast<const float4 *>(&As[kk][64 + 4 * ty]);
-        const float4 b0 = *reinterpret_cast<const float4 *>(&Bs[kk][4 * tx]);
-        const float4 b1 = *reinterpret_cast<const float4 *>(&Bs[kk][64 + 4 * tx]);
+        const float4 a0 = *reinterpret_cast<const float4 *>(&A[kk][4 * ty]);
+        const float4 a1 = *reinterpret_cast<const float4 *>(&A[kk][64 + 4 * ty]);
+        const float4 b0 = *reinterpret_cast<const float4 *>(&B[kk][4 * tx]);
+        const float4 b1 = *reinterpret_cast<const float4 *>(&B[kk][64 + 4 * tx]);
         const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
         const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
@@ -198,8 +245,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_leaf_f32(
 #pragma unroll
           for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
       }
+      // the other buffer was last read in the previous chunk, before the
+      // barrier that ended it
+      if (more) store(cur ^ 1);
+      __syncthreads();
     }
-    __syncthreads();
+    bcol = bcol_next;
+    cn = cn_next;
     // scores ||y||^2 - 2 x.y (columns past the leaf: +inf)
 #pragma unroll
     for (int i = 0; i < 8; ++i)
@@ -211,13 +263,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_leaf_f32(
       }
     __syncthreads();
     if (svalid) {
+      // a mask of the row's scores below the threshold at the tile's start
+      // (a superset of those that enter the list), then its set bits in
+      // column order, each tested again against the current threshold:
+      // the warp runs the insertion as often as its busiest lane, not once
+      // per column where any lane inserts
       const float *srow = St[sr];
       float thr = fminf(thr0, tv[KP - 1]);
-      for (int j = sp; j < cols; j += kParts) {
+      uint64_t pass = 0;
+#pragma unroll
+      for (int jj = 0; jj < kCols / kParts; ++jj) {
+        const int j = kParts * jj + sp;
+        if (srow[j] < thr && j < cols && c0 + j != my_col) pass |= 1ull << jj;
+      }
+      while (pass) {
+        const int j = kParts * (__ffsll((long long)pass) - 1) + sp;
+        pass &= pass - 1;
         const float v = srow[j];
-        const int col = c0 + j;
-        if (v < thr && col != my_col) {  // (ties with the KP-th keep the earlier column)
-          pair_insert<KP>(tv, tcol, v, col);
+        if (v < thr) {  // (ties with the KP-th keep the earlier column)
+          pair_shift_in<KP>(tv, tcol, v, c0 + j);
           thr = fminf(thr0, tv[KP - 1]);
         }
       }

@@ -466,14 +466,18 @@ __device__ __forceinline__ void key_merge_into(float *L, const float *S) {
     }
 }
 
-// L (ascending, N) <- the N smallest of L and `key`: one compare-exchange sweep.
+// L (ascending, N) <- the N smallest of L and `key`.
 template <int N>
 __device__ __forceinline__ void key_insert(float *L, float key) {
+  // entry i becomes max(old i - 1, min(old i, key)): every entry from the
+  // old list at once, no chain through the key
+  float prev = L[0];
+  L[0] = fminf(prev, key);
 #pragma unroll
-  for (int i = 0; i < N; ++i) {
-    const float lo = fminf(L[i], key);
-    key = fmaxf(L[i], key);
-    L[i] = lo;
+  for (int i = 1; i < N; ++i) {
+    const float cur = L[i];
+    L[i] = fmaxf(prev, fminf(cur, key));
+    prev = cur;
   }
 }
 
