@@ -810,12 +810,19 @@ __global__ void __launch_bounds__(MmaCfg<KP, STREAM>::threads,
         }
         (void)sc;
 #pragma unroll
-        for (int e = 0; e < kCheck; ++e) {
+        for (int e = 0; e < kCheck; e += 2) {
           const int j = h + e;
-          float sv;
-          if constexpr (FP8) sv = fmaf(m2s * sc[e], v[j], nc[e]);
-          else sv = fmaf(-2.0f, v[j], nc[e]);
-          append(aslot[j % kChains], sv, nc[e]);
+          float2 sv;
+          if constexpr (FP8) {
+            sv.x = fmaf(m2s * sc[e], v[j], nc[e]);
+            sv.y = fmaf(m2s * sc[e + 1], v[j + 1], nc[e + 1]);
+          } else {
+            // two scores per packed FP32x2 multiply-add
+            sv = fma2(make_float2(v[j], v[j + 1]), make_float2(-2.0f, -2.0f),
+                      make_float2(nc[e], nc[e + 1]));
+          }
+          append(aslot[j % kChains], sv.x, nc[e]);
+          append(aslot[(j + 1) % kChains], sv.y, nc[e + 1]);
         }
         bool over = false;
 #pragma unroll
