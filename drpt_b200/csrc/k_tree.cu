@@ -22,8 +22,8 @@
 //             double-precision interpolation of the reference
 //   count     per unit, values <= median
 //   scan      per node: unit prefix of the left counts, child offsets
-//   scatter   per unit: stable partition through shared memory, coalesced
-//             writes of the point ids and of their next-level values
+//   scatter   per unit: warp-ballot stable partition through shared memory,
+//             coalesced writes of the point ids and of their next-level values
 //
 // Every operation that the reference performs in float or double rounds on
 // its own here (__f*_rn / __d*_rn), so with exact = 1 the medians, and hence
@@ -480,11 +480,25 @@ __global__ void k_node_scan(TreeLevelArgs a) {
 }
 
 // ------------------------------------------------------------------ scatter
+// Warp-ballot stable partition of a unit through shared memory.  Position
+// p = threadIdx.x + j * kThreads is chunk c = j * kWarps + warp of 32
+// positions (so c-major order is position order); each warp's ballot of
+// "value <= median" gives the chunk's left count and, per lane, the left-goers
+// before it in the chunk; one warp scans the kUnit / 32 chunk counts.  A
+// left-goer lands at (left-goers before it), a right-goer at (left total +
+// right-goers before it): left-goers in position order, then right-goers in
+// position order.  All loads are coalesced; the point ids and their next-level
+// values then leave in coalesced writes.
 __global__ void __launch_bounds__(kThreads) k_scatter(TreeLevelArgs a) {
+  constexpr int kChunks = kUnit / 32;
+  static_assert(kChunks == 4 * 32, "one warp scans the chunk counts, four per lane");
   __shared__ int32_t sid[kUnit];
   __shared__ float sval[kUnit];
-  __shared__ int wsum[kWarps];
+  __shared__ int cbase[kChunks];  // chunk left counts, then their exclusive prefix
+  __shared__ int ltot_sh;
   const int n_units = *a.n_units;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned lt_mask = (1u << lane) - 1u;
   for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
     const int g = a.unit_node[u];
     const int t = g >> a.level;
@@ -493,47 +507,58 @@ __global__ void __launch_bounds__(kThreads) k_scatter(TreeLevelArgs a) {
     const int len = (int)min64(kUnit, r.hi - lo);
     const float *v = tree_vals(a, t) + lo;
     const float med = a.node_med[g];
-    // each thread owns kPer consecutive positions
-    const int p0 = threadIdx.x * kPer;
-    unsigned mask = 0;
-    int my = 0;
+    const int32_t *oin = a.ord_in ? a.ord_in + (int64_t)t * a.n + lo : nullptr;
+    // every value and id of the thread in flight before the ballots
+    float xs[kPer];
+    int32_t ids[kPer];
 #pragma unroll
     for (int j = 0; j < kPer; ++j) {
-      const int p = p0 + j;
-      if (p < len && __ldg(v + p) <= med) {
-        mask |= 1u << j;
-        ++my;
-      }
+      const int p = threadIdx.x + j * kThreads;
+      xs[j] = p < len ? __ldg(v + p) : 0.0f;
+      ids[j] = p < len ? (oin ? __ldg(oin + p) : (int32_t)(lo + p)) : 0;
     }
-    // exclusive scan of the per-thread left counts
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int x = my;
+    unsigned bal[kPer];
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(kFull, x, o);
-      if (lane >= o) x += y;
+    for (int j = 0; j < kPer; ++j) {
+      const int p = threadIdx.x + j * kThreads;
+      bal[j] = __ballot_sync(kFull, p < len && xs[j] <= med);  // drpt_global.cpp:308
+      if (lane == 0) cbase[j * kWarps + w] = __popc(bal[j]);
     }
-    if (lane == 31) wsum[w] = x;
     __syncthreads();
-    int wbase = 0, ltot = 0;
-    for (int k = 0; k < kWarps; ++k) {
-      if (k < w) wbase += wsum[k];
-      ltot += wsum[k];
+    if (w == 0) {
+      int c4[4], sum = 0;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        c4[e] = cbase[4 * lane + e];
+        sum += c4[e];
+      }
+      int x = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+      }
+      int run = x - sum;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        cbase[4 * lane + e] = run;
+        run += c4[e];
+      }
+      if (lane == 31) ltot_sh = x;
     }
-    int lrank = wbase + x - my;            // left-goers before p0 in the unit
-    int rrank = ltot + (p0 - lrank);       // slot of this thread's first right-goer
-    const int32_t *oin = a.ord_in ? a.ord_in + (int64_t)t * a.n + lo : nullptr;
+    __syncthreads();
+    const int ltot = ltot_sh;
     const bool want_val = a.val_out != nullptr;
     const float *pnext =
         want_val ? a.P + ((int64_t)t * (a.gd - 1) + a.level - a.p_level0 + 1) * a.n : nullptr;
 #pragma unroll
     for (int j = 0; j < kPer; ++j) {
-      const int p = p0 + j;
+      const int p = threadIdx.x + j * kThreads;
       if (p < len) {
-        const int32_t id = oin ? __ldg(oin + p) : (int32_t)(lo + p);
-        const int slot = ((mask >> j) & 1u) ? lrank++ : rrank++;
-        sid[slot] = id;
-        if (want_val) sval[slot] = __ldg(pnext + id);
+        const int lbefore = cbase[j * kWarps + w] + __popc(bal[j] & lt_mask);
+        const int slot = ((bal[j] >> lane) & 1u) ? lbefore : ltot + (p - lbefore);
+        sid[slot] = ids[j];
+        if (want_val) sval[slot] = __ldg(pnext + ids[j]);
       }
     }
     __syncthreads();
@@ -547,7 +572,7 @@ __global__ void __launch_bounds__(kThreads) k_scatter(TreeLevelArgs a) {
       oout[dst] = sid[i];
       if (want_val) vout[dst] = sval[i];
     }
-    __syncthreads();  // sid, sval and wsum are reused by the next unit
+    __syncthreads();  // sid, sval and cbase are reused by the next unit
   }
 }
 
