@@ -197,6 +197,30 @@ __global__ void __launch_bounds__(256) k_leaf_mean(const T *__restrict__ X, int6
 // with saturation (d_pad bytes, zero-padded); the scale goes to `scl`.  In
 // both cases `nrm` receives the squared norm of the row the tensor cores see
 // (dequantised for FP8), so that ||y||^2 - 2 x.y ranks the same values.
+// Sums of RB (a power of two, <= 32) per-lane values s[q] over the warp, all
+// at once: while more than one value is left, each lane keeps half of its
+// values and sends the other half to the lane that keeps those (log2 RB
+// steps of RB/2, ..., 1 shuffles), then a plain butterfly over the lanes
+// that hold the same value.  Lane l returns the sum for q = l >> (5 - log2 RB).
+template <int RB>
+__device__ __forceinline__ float warp_sum_rows(float *s, int lane) {
+  int bit = 16;
+#pragma unroll
+  for (int cnt = RB; cnt > 1; cnt >>= 1, bit >>= 1) {
+    const bool up = (lane & bit) != 0;
+#pragma unroll
+    for (int i = 0; i < cnt / 2; ++i) {
+      const float keep = up ? s[i + cnt / 2] : s[i];
+      const float send = up ? s[i] : s[i + cnt / 2];
+      s[i] = keep + __shfl_xor_sync(kFull, send, bit);
+    }
+  }
+  float v = s[0];
+#pragma unroll
+  for (int o = bit; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
 template <int NCH>
 struct StageCfg {
   static constexpr int rb = NCH <= 2 ? 4 / NCH : 1;           // points per warp step
@@ -258,8 +282,10 @@ __global__ void __launch_bounds__(256, StageCfg<NCH>::min_blocks) k_leaf_stage(c
             if (FULL || c0 < d) load4<float>(mr + c0, m4[q][h]);
           }
         }
+        float sqs[RB];  // BF16: this lane's part of each point's squared norm
 #pragma unroll
         for (int q = 0; q < RB; ++q) {
+          sqs[q] = 0.0f;
           const int32_t row = rows[q];
           if (row < 0) continue;  // warp-uniform: a point past the end
           float c[NCH][4];
@@ -323,9 +349,17 @@ __global__ void __launch_bounds__(256, StageCfg<NCH>::min_blocks) k_leaf_stage(c
                 __stcs(reinterpret_cast<uint2 *>(dst + c0), *reinterpret_cast<const uint2 *>(b));
               }
             }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(kFull, sq, o);
-            if (lane == 0) __stcs(nrm + orow, sq);
+            sqs[q] = sq;
+          }
+        }
+        if constexpr (!FP8) {
+          // the RB norms summed over the warp together: lane l ends with
+          // point (l >> (5 - log2 RB)); the first lane of each group stores it
+          const float nv = warp_sum_rows<RB>(sqs, lane);
+          constexpr int kGroup = 32 / RB;
+          if ((lane & (kGroup - 1)) == 0) {
+            const int32_t row = rows[lane / kGroup];
+            if (row >= 0) __stcs(nrm + (int64_t)t * n + row, nv);
           }
         }
       }
