@@ -83,10 +83,28 @@ TREES_MIXED = (f"mixed form: {MIXED_TREES} trees, global leaves of about {MIXED_
 TREES_REFERENCE = (f"reference parameters: {NTREES} trees, tree depth int(log2 n - 2), ratio 0.6, "
                    "positional local split")
 # The reference's cblas calls (sgemm of the projection, saxpy/snrm2 of its
-# distance) run in the project's ordered cblas (plain loops in a fixed
-# summation order, oracle/refbuild/cblas_ordered.cpp): the host has no
-# OpenBLAS, the library the reference's CMake file names.
-REF_CBLAS = "ordered cblas (plain loops, oracle/refbuild/cblas_ordered.cpp); no OpenBLAS on the host"
+# distance) run in OpenBLAS, the library its build names: numpy's bundled
+# scipy-openblas (oracle/_ref/drpt_ref_openblas, `make -C oracle
+# ref-openblas`).  Without that build they run in the project's ordered cblas
+# (plain loops in a fixed summation order, oracle/refbuild/cblas_ordered.cpp),
+# the build the parity tests use.
+REF_BINARIES = (("drpt_ref_openblas", "OpenBLAS (numpy's bundled scipy-openblas, "
+                 "oracle/refbuild/cblas_openblas.cpp)"),
+                ("drpt_ref", "ordered cblas (plain loops, oracle/refbuild/cblas_ordered.cpp)"))
+
+
+def _reference_cblas() -> str:
+    found = _reference_binary()
+    return found[1] if found else "none (the CPU restatement was timed)"
+
+
+def _reference_binary():
+    """(path, cblas description) of the reference build to time, or None."""
+    for name, cblas in REF_BINARIES:
+        path = os.path.join(ROOT, "oracle", "_ref", name)
+        if os.path.exists(path):
+            return path, cblas
+    return None
 
 
 def _env_int(name, default):
@@ -175,15 +193,16 @@ def run_reference_once(path: str, n: int, threads: int, dump: str | None = None)
     """One run of the reference binary; returns (build_s, query_s, kind).
     `dump`: a file for its merged neighbour lists (written after the timed
     phases)."""
-    ref = os.path.join(ROOT, "oracle", "_ref", "drpt_ref")
+    found = _reference_binary()
     seeds = ",".join(str(s) for s in [SEED_PROJ] + list(range(1, NTREES + 1)))
-    if os.path.exists(ref):
+    if found:
+        ref = found[0]
         out_dir = tempfile.mkdtemp()
         cmd = (f"ulimit -s unlimited; exec {ref} -input {path} -output {out_dir}/ -data-set-size {n} "
                f"-dimension {DIM} -ntrees {NTREES} -nn {NN} -locality 0 -data-file-format 1 -no-write"
                + (f" -dump {dump}" if dump else ""))
         env = dict(os.environ, DRPT_REF_SEEDS=seeds, OMP_NUM_THREADS=str(threads),
-                   OMP_PROC_BIND="true")
+                   OPENBLAS_NUM_THREADS=str(threads), OMP_PROC_BIND="true")
         r = subprocess.run(["bash", "-c", cmd], env=env, capture_output=True, text=True)
         shutil.rmtree(out_dir, ignore_errors=True)
         m = re.search(r"Index building \(s\)\s*([0-9.eE+-]+)\s*Querying Time \(s\)\s*([0-9.eE+-]+)",
@@ -229,7 +248,8 @@ def cpu_baseline(n: int = CPU_SAMPLE):
             "kind": kind,
             "sample": f"{n} points of the same distribution (clusters scaled to {max(1, round(N_CLUSTERS * n / N_POINTS))}), "
                       f"{TREES_REFERENCE}, nn={NN}, 1 rank x {threads if kind == 'reference' else 1} threads; "
-                      f"time = index building + querying ({b:.2f} s + {q:.2f} s); {REF_CBLAS}",
+                      f"time = index building + querying ({b:.2f} s + {q:.2f} s); "
+                      f"cblas: {_reference_cblas()}",
             "recall@10": rec}
 
 
@@ -263,7 +283,7 @@ def reference_arm(args):
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "trees": TREES_REFERENCE, "ntrees": NTREES,
                    "sample_points": REF_STEP_SAMPLE, "ranks": 1, "threads": threads,
-                   "recall@10": rec, "recall_sample": 1000, "cblas": REF_CBLAS,
+                   "recall@10": rec, "recall_sample": 1000, "cblas": _reference_cblas(),
                    "note": "the sample is bounded so that the run ends in minutes; the "
                            "reference's recall depends on its thread count (the order of "
                            "points inside a node feeds its positional local split)"},

@@ -17,6 +17,7 @@ from __future__ import annotations
 import ctypes
 import os
 import subprocess
+import sys
 
 import numpy as np
 
@@ -44,7 +45,8 @@ def build_lib(reference_root: str | None = None) -> None:
     """Compile libdrpt_oracle.so with the recipe in oracle/Makefile and, when
     a reference checkout is named (`reference_root`, else the environment's
     DRPT_REFERENCE_ROOT), the reference binary _ref/drpt_ref from its
-    sources and, once libdrpt_gpu.so exists, the reference-side binding's
+    sources (and _ref/drpt_ref_openblas, the same on OpenBLAS, for timing)
+    and, once libdrpt_gpu.so exists, the reference-side binding's
     test driver _ref/adapter_check.  A named root that is not a directory is an error; with none
     named the reference binary is not built."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
@@ -54,6 +56,10 @@ def build_lib(reference_root: str | None = None) -> None:
     if not os.path.isdir(root):
         raise FileNotFoundError(f"reference checkout {root!r} (DRPT_REFERENCE_ROOT) not found")
     subprocess.run(["make", "-s", "-C", HERE, "ref", "REF_ROOT=" + root], check=True)
+    # the same build on OpenBLAS (numpy's bundled copy), for the timed CPU
+    # baseline only; skipped where numpy ships no OpenBLAS
+    subprocess.run(["make", "-s", "-C", HERE, "ref-openblas", "REF_ROOT=" + root,
+                    "PYTHON=" + sys.executable], check=False)
     # the reference-side binding of the library, where the library is built
     if os.path.exists(os.path.join(os.path.dirname(HERE), "drpt_b200", "libdrpt_gpu.so")):
         subprocess.run(["make", "-s", "-C", HERE, "adapter", "REF_ROOT=" + root], check=True)
