@@ -98,11 +98,21 @@ def _reference_cblas() -> str:
     return found[1] if found else "none (the CPU restatement was timed)"
 
 
+def _loads(path: str) -> bool:
+    """True unless the dynamic loader reports a missing library for `path`."""
+    try:
+        r = subprocess.run(["ldd", path], capture_output=True, text=True, timeout=30)
+    except (OSError, subprocess.SubprocessError):
+        return True  # no ldd: let the run itself report a failure
+    return "not found" not in r.stdout
+
+
 def _reference_binary():
-    """(path, cblas description) of the reference build to time, or None."""
+    """(path, cblas description) of the reference build to time, or None:
+    the OpenBLAS build where its library loads, else the ordered-cblas one."""
     for name, cblas in REF_BINARIES:
         path = os.path.join(ROOT, "oracle", "_ref", name)
-        if os.path.exists(path):
+        if os.path.exists(path) and _loads(path):
             return path, cblas
     return None
 
