@@ -71,13 +71,19 @@ __device__ void node_bounds(float mu, float sigma, float *D) {
 // decrease (offsets from the mean in increasing order, rounded
 // monotonically) and D[14] = D[15] = 0, so for x <= D[13] the slot is the
 // number of D[0..12] below x (0 when x <= D[0], and for a NaN x); above
-// D[13] only slot 14 can take x, when x <= 0.
+// D[13] only slot 14 can take x, when x <= 0.  That count is found by a
+// branch-free binary search over D[0..12] (a lower bound in a non-decreasing
+// array; D[13] >= x closes it): four compares instead of thirteen, the same
+// slot for every x, NaNs included (every compare with a NaN is false).
 __device__ __forceinline__ int bin_of(const float *D, float x) {
   if (x > D[13]) return x <= 0.0f ? 14 : 0;
-  int slot = 0;
-#pragma unroll
-  for (int j = 0; j < 13; ++j) slot += D[j] < x ? 1 : 0;
-  return slot;
+  const bool c8 = D[7] < x;                                              // >= 8 below
+  const bool c4 = (c8 ? D[11] : D[3]) < x;                               // + 4
+  const bool c2 = (c8 ? (c4 ? D[13] : D[9]) : (c4 ? D[5] : D[1])) < x;  // + 2
+  const int s = (c8 ? 8 : 0) + (c4 ? 4 : 0) + (c2 ? 2 : 0);
+  const float t = c8 ? (c4 ? D[12] : (c2 ? D[10] : D[8]))
+                     : (c4 ? (c2 ? D[6] : D[4]) : (c2 ? D[2] : D[0]));
+  return s + (t < x ? 1 : 0);                                           // + 1
 }
 
 // Median selection and interpolation (math_operations.cpp:333-375): the
@@ -325,9 +331,10 @@ __global__ void k_bounds_fast(TreeLevelArgs a) {
 }
 
 // ------------------------------------------------------------------ histogram
-// Per thread, the 16 counts are 16-bit fields of four 64-bit registers
-// (at most kPer values per thread and kUnit per warp sum, both below 2^16),
-// added over the warp with shuffles; no atomics.
+// Per thread, the 16 counts are 8-bit fields of two 64-bit registers (at
+// most kPer = 16 values per thread), widened to 16-bit fields of four
+// registers (a warp's sum is at most 512) and added over the warp with
+// shuffles; no atomics.
 __global__ void __launch_bounds__(kThreads) k_hist(TreeLevelArgs a) {
   __shared__ unsigned hist[kWarps][kBins];
   __shared__ float Ds[kBins];
@@ -345,7 +352,8 @@ __global__ void __launch_bounds__(kThreads) k_hist(TreeLevelArgs a) {
 #pragma unroll
     for (int j = 0; j < kBins; ++j) D[j] = Ds[j];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint64_t c4[4] = {0ull, 0ull, 0ull, 0ull};
+    static_assert(kPer < 256, "a thread's counts fit 8-bit fields");
+    uint64_t c2[2] = {0ull, 0ull};
     float xs[kPer];
 #pragma unroll
     for (int j = 0; j < kPer; ++j) {
@@ -356,10 +364,18 @@ __global__ void __launch_bounds__(kThreads) k_hist(TreeLevelArgs a) {
     for (int j = 0; j < kPer; ++j) {
       if (threadIdx.x + j * kThreads < len) {
         const int b = bin_of(D, xs[j]);
-        const uint64_t inc = 1ull << (16 * (b & 3));
-#pragma unroll
-        for (int q = 0; q < 4; ++q) c4[q] += (b >> 2) == q ? inc : 0ull;
+        const uint64_t inc = 1ull << (8 * (b & 7));
+        c2[0] += b < 8 ? inc : 0ull;
+        c2[1] += b < 8 ? 0ull : inc;
       }
+    }
+    // bins 4q .. 4q + 3 as 16-bit fields of c4[q]
+    uint64_t c4[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t x = (uint32_t)(c2[q >> 1] >> (32 * (q & 1)));
+      c4[q] = (uint64_t)(x & 0xffu) | ((uint64_t)((x >> 8) & 0xffu) << 16) |
+              ((uint64_t)((x >> 16) & 0xffu) << 32) | ((uint64_t)(x >> 24) << 48);
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q)
