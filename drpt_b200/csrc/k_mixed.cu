@@ -292,9 +292,22 @@ __global__ void __launch_bounds__(256, StageCfg<NCH>::min_blocks) k_leaf_stage(c
 #pragma unroll
           for (int h = 0; h < NCH; ++h) {
             const int c0 = h * 128 + 4 * lane;
+            if constexpr (FULL) {
+              // two differences per packed FP32x2 multiply-add (-1 * m + v,
+              // one rounding: the same value as v - m)
 #pragma unroll
-            for (int e = 0; e < 4; ++e)
-              c[h][e] = (FULL || c0 + e < d) ? v[q][h][e] - m4[q][h][e] : 0.0f;
+              for (int e = 0; e < 4; e += 2) {
+                const float2 r = fma2(make_float2(m4[q][h][e], m4[q][h][e + 1]),
+                                      make_float2(-1.0f, -1.0f),
+                                      make_float2(v[q][h][e], v[q][h][e + 1]));
+                c[h][e] = r.x;
+                c[h][e + 1] = r.y;
+              }
+            } else {
+#pragma unroll
+              for (int e = 0; e < 4; ++e)
+                c[h][e] = c0 + e < d ? v[q][h][e] - m4[q][h][e] : 0.0f;
+            }
           }
           const int64_t orow = (int64_t)t * n + row;
           float sq = 0.0f;
@@ -335,21 +348,25 @@ __global__ void __launch_bounds__(256, StageCfg<NCH>::min_blocks) k_leaf_stage(c
             }
           } else {
             __nv_bfloat16 *dst = static_cast<__nv_bfloat16 *>(Xq) + orow * d_pad;
+            // squares of the rounded values, even and odd dimensions in the
+            // two halves of a packed FP32x2 sum
+            float2 sq2 = make_float2(0.0f, 0.0f);
 #pragma unroll
             for (int h = 0; h < NCH; ++h) {
               const int c0 = h * 128 + 4 * lane;
               if (FULL || c0 < d_pad) {
-                __nv_bfloat16 b[4];
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                  b[e] = __float2bfloat16_rn(c[h][e]);
-                  const float vr = __bfloat162float(b[e]);
-                  sq = fmaf(vr, vr, sq);
-                }
-                __stcs(reinterpret_cast<uint2 *>(dst + c0), *reinterpret_cast<const uint2 *>(b));
+                const __nv_bfloat162 b01 = __floats2bfloat162_rn(c[h][0], c[h][1]);
+                const __nv_bfloat162 b23 = __floats2bfloat162_rn(c[h][2], c[h][3]);
+                const float2 r01 = __bfloat1622float2(b01), r23 = __bfloat1622float2(b23);
+                sq2 = fma2(r01, r01, sq2);
+                sq2 = fma2(r23, r23, sq2);
+                uint2 pk;
+                pk.x = *reinterpret_cast<const uint32_t *>(&b01);
+                pk.y = *reinterpret_cast<const uint32_t *>(&b23);
+                __stcs(reinterpret_cast<uint2 *>(dst + c0), pk);
               }
             }
-            sqs[q] = sq;
+            sqs[q] = sq2.x + sq2.y;
           }
         }
         if constexpr (!FP8) {
