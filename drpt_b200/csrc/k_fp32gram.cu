@@ -1,10 +1,11 @@
 // FP32 CUDA-core form of the whole-leaf brute force (DRPT_MODE_FP32_GRAM):
 // the same trees, running list and exact FP32 re-rank as the mixed form, with
 // the leaf Gram tiles computed in FP32 by fused multiply-adds on the CUDA
-// cores instead of BF16 tiles on the tensor cores.  It is the fastest plain
-// FP32 counterpart of the mixed form (the reference's own per-pair
-// subtract / multiply / add sequence, kept bit for bit by k_leaf_knn, takes
-// three FP32 operations per dimension and pair; this takes one).
+// cores (packed FP32x2 multiply-adds) instead of BF16 tiles on the tensor
+// cores.  It is the fastest plain FP32 counterpart of the mixed form (the
+// reference's own per-pair subtract / multiply / add sequence, kept bit for
+// bit by k_leaf_knn, takes three FP32 operations per dimension and pair; this
+// takes one).
 //
 //   k_row_norms   ||x||^2 of every row in FP32 (once per build)
 //   k_leaf_f32    per CTA one 128-row tile of a global leaf against every
@@ -23,6 +24,7 @@
 // Reference: the leaf brute force MDRPT::calculate_nns (mdrpt.cpp:123-212)
 // with MathOp::calculate_distance (math_operations.cpp:385-396).
 #include "kernels.cuh"
+#include "sm100.cuh"
 
 namespace drpt {
 namespace {
@@ -240,10 +242,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_leaf_f32(
         const float4 b1 = *reinterpret_cast<const float4 *>(&B[kk][64 + 4 * tx]);
         const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
         const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        // two columns per packed FP32x2 multiply-add (each product rounded
+        // once into its own sum, in the same order as scalar FMAs)
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+        for (int i = 0; i < 8; ++i) {
+          const float2 ai = make_float2(av[i], av[i]);
 #pragma unroll
-          for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+          for (int j = 0; j < 8; j += 2) {
+            const float2 r = sm100::fma2(ai, make_float2(bv[j], bv[j + 1]),
+                                         make_float2(acc[i][j], acc[i][j + 1]));
+            acc[i][j] = r.x;
+            acc[i][j + 1] = r.y;
+          }
+        }
       }
       // the other buffer was last read in the previous chunk, before the
       // barrier that ended it
